@@ -1,0 +1,96 @@
+/*
+ * tsdx_cuda.h — C-ABI of the B200 (sm_100a) batched small-matrix solver.
+ *
+ * This is the drop-in boundary behind TinySolverDx's batched API. Every entry
+ * point takes plain pointers and sizes and returns an int status (0 = success,
+ * negative = error, see TSDX_ERR_*); numerical failure is never an error but a
+ * LAPACK-style info code, exactly as in the reference.
+ *
+ * Layouts (TinySolverDx include/tinysolverdx/batched.hpp:1-6, :247):
+ *   A    (batch, n, n)   row-major, matrices contiguous; overwritten by the factor
+ *   B    (batch, n, nrhs) row-major; overwritten by the solution
+ *   piv  (batch, n) int32, 0-based LAPACK sequential pivots (piv[k] = row swapped with k)
+ *   info (batch) int32 or NULL: 0 ok, k > 0 first failing pivot (1-based)
+ * Sizes: 1 <= n <= 64, batch >= 0, nrhs >= 0.
+ *
+ * Two families:
+ *  - tsdx_cuda_*      : DEVICE pointers, asynchronous on `stream` (a cudaStream_t
+ *                       passed as void*, NULL = the legacy default stream).
+ *  - tsdx_cuda_*_host : HOST pointers, synchronous, same semantics as the
+ *                       reference's CUDA backend (copy in, compute, copy out).
+ *
+ * Numerical contract: Cholesky factors, LU factors, pivots and info are
+ * bit-identical to the reference CPU library's default backends (Cholesky:
+ * kernels.hpp:57-87 as the simd backend compiles it; LU: kernels.hpp:91-119);
+ * solutions agree to rounding (column-oriented back substitution).
+ */
+#ifndef TSDX_CUDA_H
+#define TSDX_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TSDX_OK 0
+#define TSDX_ERR_N (-1)     /* n outside [1, 64] (batched.hpp:39-41)              */
+#define TSDX_ERR_BATCH (-2) /* batch < 0 (batched.hpp:42)                          */
+#define TSDX_ERR_NULL (-3)  /* a required pointer is NULL (batched.hpp:184 for piv) */
+#define TSDX_ERR_NRHS (-4)  /* nrhs < 0                                            */
+#define TSDX_ERR_CUDA (-5)  /* a CUDA runtime call failed; see tsdx_cuda_last_error */
+#define TSDX_ERR_NODEV (-6) /* no CUDA device is visible                           */
+
+/* 1 if a CUDA device is visible (replaces tsdx::cuda::available, cuda_backend.hpp:9). */
+int tsdx_cuda_available(void);
+/* Message of the last TSDX_ERR_CUDA on the calling thread ("" if none). */
+const char* tsdx_cuda_last_error(void);
+/* Kernels of this library launched since load (all threads); for accounting. */
+int64_t tsdx_cuda_launch_count(void);
+
+/* ---- device-pointer, stream-ordered API ---------------------------------------
+ * potrf  replaces cholesky_batched<T>(A, n, batch, info, Backend::Cuda)  batched.hpp:121-133
+ * getrf  replaces lu_batched<T>(A, n, batch, piv, info, Backend::Cuda)    batched.hpp:181-197
+ * potrs  replaces cholesky_solve_batched<T>(L, n, batch, B, nrhs)         batched.hpp:248-257
+ * getrs  replaces lu_solve_batched<T>(LU, piv, n, batch, B, nrhs)         batched.hpp:259-268
+ * posv   replaces posv_batched<T>(A, n, batch, B, nrhs, info, be)         batched.hpp:271-275
+ * gesv   replaces gesv_batched<T>(A, n, batch, B, nrhs, piv, info, be)    batched.hpp:276-280
+ */
+int tsdx_cuda_potrf_f32(float* A, int n, int64_t batch, int* info, void* stream);
+int tsdx_cuda_potrf_f64(double* A, int n, int64_t batch, int* info, void* stream);
+int tsdx_cuda_getrf_f32(float* A, int n, int64_t batch, int* piv, int* info, void* stream);
+int tsdx_cuda_getrf_f64(double* A, int n, int64_t batch, int* piv, int* info, void* stream);
+int tsdx_cuda_potrs_f32(const float* L, int n, int64_t batch, float* B, int nrhs, void* stream);
+int tsdx_cuda_potrs_f64(const double* L, int n, int64_t batch, double* B, int nrhs, void* stream);
+int tsdx_cuda_getrs_f32(const float* LU, const int* piv, int n, int64_t batch, float* B, int nrhs, void* stream);
+int tsdx_cuda_getrs_f64(const double* LU, const int* piv, int n, int64_t batch, double* B, int nrhs, void* stream);
+int tsdx_cuda_posv_f32(float* A, int n, int64_t batch, float* B, int nrhs, int* info, void* stream);
+int tsdx_cuda_posv_f64(double* A, int n, int64_t batch, double* B, int nrhs, int* info, void* stream);
+int tsdx_cuda_gesv_f32(float* A, int n, int64_t batch, float* B, int nrhs, int* piv, int* info, void* stream);
+int tsdx_cuda_gesv_f64(double* A, int n, int64_t batch, double* B, int nrhs, int* piv, int* info, void* stream);
+
+/* ---- host-pointer, synchronous API ---------------------------------------------
+ * cholesky_batched_host / lu_batched_host replace tsdx::cuda::cholesky_batched /
+ * tsdx::cuda::lu_batched (cuda_backend.hpp:10-11, cuda_backend.cu:155-188); the
+ * solve and one-shot forms extend Backend::Cuda to the solves, which the
+ * reference always runs on the CPU (batched.hpp:249, :260). Large batches are
+ * streamed through the device in chunks so that the copies overlap the kernels.
+ */
+int tsdx_cuda_cholesky_batched_host_f32(float* A, int n, int64_t batch, int* info);
+int tsdx_cuda_cholesky_batched_host_f64(double* A, int n, int64_t batch, int* info);
+int tsdx_cuda_lu_batched_host_f32(float* A, int n, int64_t batch, int* piv, int* info);
+int tsdx_cuda_lu_batched_host_f64(double* A, int n, int64_t batch, int* piv, int* info);
+int tsdx_cuda_cholesky_solve_batched_host_f32(const float* L, int n, int64_t batch, float* B, int nrhs);
+int tsdx_cuda_cholesky_solve_batched_host_f64(const double* L, int n, int64_t batch, double* B, int nrhs);
+int tsdx_cuda_lu_solve_batched_host_f32(const float* LU, const int* piv, int n, int64_t batch, float* B, int nrhs);
+int tsdx_cuda_lu_solve_batched_host_f64(const double* LU, const int* piv, int n, int64_t batch, double* B, int nrhs);
+int tsdx_cuda_posv_batched_host_f32(float* A, int n, int64_t batch, float* B, int nrhs, int* info);
+int tsdx_cuda_posv_batched_host_f64(double* A, int n, int64_t batch, double* B, int nrhs, int* info);
+int tsdx_cuda_gesv_batched_host_f32(float* A, int n, int64_t batch, float* B, int nrhs, int* piv, int* info);
+int tsdx_cuda_gesv_batched_host_f64(double* A, int n, int64_t batch, double* B, int nrhs, int* piv, int* info);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TSDX_CUDA_H */

@@ -1,0 +1,40 @@
+"""The C-ABI library loads without a GPU, exports every symbol include/tsdx_cuda.h
+declares, and rejects bad arguments before touching a device (the reference's
+batched.hpp:39-43, :184 validation)."""
+import ctypes as C
+import re
+
+import numpy as np
+
+from conftest import ROOT, load_pkg
+
+capi = load_pkg("capi")
+
+
+def declared_symbols():
+    text = (ROOT / "include" / "tsdx_cuda.h").read_text()
+    return sorted(set(re.findall(r"\b(tsdx_cuda_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = capi.lib()
+    names = declared_symbols()
+    assert len(names) >= 27
+    for name in names:
+        assert hasattr(lib, name), name
+    assert set(names) >= set(capi.SIGNATURES)
+
+
+def test_validation_without_device():
+    lib = capi.lib()
+    A = np.zeros((2, 4, 4))
+    info = np.zeros(2, np.int32)
+    piv = np.zeros((2, 4), np.int32)
+    assert lib.tsdx_cuda_cholesky_batched_host_f64(capi.ptr(A), 0, 2, capi.ptr(info)) == capi.TSDX_ERR_N
+    assert lib.tsdx_cuda_cholesky_batched_host_f64(capi.ptr(A), 65, 2, capi.ptr(info)) == capi.TSDX_ERR_N
+    assert lib.tsdx_cuda_cholesky_batched_host_f64(capi.ptr(A), 4, -1, capi.ptr(info)) == capi.TSDX_ERR_BATCH
+    assert lib.tsdx_cuda_lu_batched_host_f64(capi.ptr(A), 4, 2, None, capi.ptr(info)) == capi.TSDX_ERR_NULL
+    assert lib.tsdx_cuda_posv_batched_host_f64(capi.ptr(A), 4, 2, capi.ptr(A), -1, capi.ptr(info)) == capi.TSDX_ERR_NRHS
+    # an empty batch is a successful no-op (batched.hpp:126)
+    assert lib.tsdx_cuda_lu_batched_host_f64(capi.ptr(A), 4, 0, capi.ptr(piv), capi.ptr(info)) == capi.TSDX_OK
+    assert lib.tsdx_cuda_getrf_f32(None, 4, 0, None, None, None) == capi.TSDX_ERR_NULL

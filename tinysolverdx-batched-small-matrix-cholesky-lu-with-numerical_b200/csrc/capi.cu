@@ -1,0 +1,260 @@
+// C-ABI of the batched solver (declared in include/tsdx_cuda.h).
+//
+// Device-pointer entry points validate their arguments exactly like the
+// reference's batch drivers (batched.hpp:39-43, :184) and enqueue one fused
+// kernel per pass of at most 8 right-hand sides. Host-pointer entry points
+// replace the reference's synchronous CUDA backend (cuda_backend.cu:155-188):
+// they stream the batch through a cached device workspace in chunks, with the
+// host->device copy of one chunk, the kernel of the previous one and the
+// device->host copy of the one before that in flight at the same time.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "../../include/tsdx_cuda.h"
+#include "launch.cuh"
+
+namespace tsdx {
+namespace host {
+
+namespace {
+thread_local std::string g_err;
+std::atomic<long long> g_launches{0};
+int g_sms[64] = {0};
+}  // namespace
+
+void set_cuda_error(cudaError_t e, const char* what) {
+  g_err = std::string(what) + ": " + cudaGetErrorString(e);
+}
+std::atomic<long long>& launch_counter() { return g_launches; }
+
+int device_sms(int dev) {
+  if (dev < 0 || dev >= 64) return 148;
+  if (g_sms[dev] == 0) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+    g_sms[dev] = v;
+  }
+  return g_sms[dev];
+}
+
+namespace {
+
+enum Kind { POTRF, GETRF, POTRS, GETRS, POSV, GESV };
+
+inline int check_common(int n, int64_t batch, int nrhs) {
+  if (n < 1 || n > 64) return TSDX_ERR_N;
+  if (batch < 0) return TSDX_ERR_BATCH;
+  if (nrhs < 0) return TSDX_ERR_NRHS;
+  return TSDX_OK;
+}
+template <class T> inline bool aligned(const T* p) { return reinterpret_cast<uintptr_t>(p) % alignof(T) == 0; }
+
+// ---- device-pointer implementation --------------------------------------------
+template <class T>
+int run_device(Kind kind, T* A, const int* piv_in, int n, int64_t batch, T* B, int nrhs, int* piv, int* info,
+               cudaStream_t st) {
+  if (int rc = check_common(n, batch, nrhs)) return rc;
+  const bool has_b = (kind == POTRS || kind == GETRS || kind == POSV || kind == GESV);
+  if (!has_b) nrhs = 0;
+  if (!A || !aligned(A)) return TSDX_ERR_NULL;
+  if ((kind == GETRF || kind == GESV) && !piv) return TSDX_ERR_NULL;
+  if (kind == GETRS && !piv_in) return TSDX_ERR_NULL;
+  if (has_b && nrhs > 0 && (!B || !aligned(B))) return TSDX_ERR_NULL;
+  if (batch == 0) return TSDX_OK;
+
+  dev::SolveArgs<T> a{};
+  a.A = A;
+  a.B = B;
+  a.piv = (kind == GETRS) ? const_cast<int*>(piv_in) : piv;
+  a.info = info;
+  a.batch = batch;
+  a.n = n;
+  a.ldb = nrhs;
+  if (kind == POTRF || kind == GETRF || kind == POSV || kind == GESV) {
+    a.b0 = 0;
+    a.nrhs = std::min(nrhs, 8);
+    const int rc = (kind == POTRF || kind == POSV) ? run_chol<T>(a, st) : run_lu<T>(a, st);
+    if (rc) return rc;
+    for (int b0 = 8; b0 < nrhs; b0 += 8) {  // remaining right-hand sides from the factor
+      a.b0 = b0;
+      a.nrhs = std::min(8, nrhs - b0);
+      const int r2 = (kind == POSV) ? run_potrs<T>(a, st) : run_getrs<T>(a, st);
+      if (r2) return r2;
+    }
+    return TSDX_OK;
+  }
+  for (int b0 = 0; b0 < nrhs; b0 += 8) {
+    a.b0 = b0;
+    a.nrhs = std::min(8, nrhs - b0);
+    const int rc = (kind == POTRS) ? run_potrs<T>(a, st) : run_getrs<T>(a, st);
+    if (rc) return rc;
+  }
+  return TSDX_OK;
+}
+
+// ---- host-pointer implementation ----------------------------------------------
+constexpr int kSlots = 3;
+constexpr size_t kChunkBytes = size_t(96) << 20;  // A bytes per chunk
+
+struct Slot {
+  void* a = nullptr;
+  void* b = nullptr;
+  int* piv = nullptr;
+  int* info = nullptr;
+  size_t acap = 0, bcap = 0, pcap = 0, icap = 0;
+  cudaStream_t st = nullptr;
+};
+struct DeviceCtx {
+  Slot slot[kSlots];
+  bool init = false;
+};
+std::mutex g_host_mu;
+DeviceCtx g_ctx[64];
+
+int grow(void** p, size_t* cap, size_t need) {
+  if (need <= *cap) return 0;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  cudaError_t e = cudaMalloc(p, need);
+  if (e != cudaSuccess) { set_cuda_error(e, "cudaMalloc"); return TSDX_ERR_CUDA; }
+  *cap = need;
+  return 0;
+}
+
+#define TSDX_CK(call, what)                                          \
+  do {                                                               \
+    cudaError_t e_ = (call);                                         \
+    if (e_ != cudaSuccess) { set_cuda_error(e_, what); return TSDX_ERR_CUDA; } \
+  } while (0)
+
+template <class T>
+int run_host(Kind kind, T* A, const int* piv_in, int n, int64_t batch, T* B, int nrhs, int* piv, int* info) {
+  if (int rc = check_common(n, batch, nrhs)) return rc;
+  const bool has_b = (kind == POTRS || kind == GETRS || kind == POSV || kind == GESV);
+  if (!has_b) nrhs = 0;
+  if (!A) return TSDX_ERR_NULL;
+  if ((kind == GETRF || kind == GESV) && !piv) return TSDX_ERR_NULL;
+  if (kind == GETRS && !piv_in) return TSDX_ERR_NULL;
+  if (has_b && nrhs > 0 && !B) return TSDX_ERR_NULL;
+  if (batch == 0) return TSDX_OK;
+  int devi = 0;
+  if (cudaGetDevice(&devi) != cudaSuccess) return TSDX_ERR_NODEV;
+  if (devi >= 64) return TSDX_ERR_NODEV;
+
+  std::lock_guard<std::mutex> lock(g_host_mu);
+  DeviceCtx& ctx = g_ctx[devi];
+  if (!ctx.init) {
+    for (auto& s : ctx.slot) TSDX_CK(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking), "cudaStreamCreate");
+    ctx.init = true;
+  }
+  const size_t mat = size_t(n) * n * sizeof(T), rhs = size_t(n) * nrhs * sizeof(T);
+  const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(batch, int64_t(kChunkBytes / mat)));
+  for (auto& s : ctx.slot) {
+    if (int rc = grow(&s.a, &s.acap, mat * chunk)) return rc;
+    if (has_b && nrhs > 0)
+      if (int rc = grow(&s.b, &s.bcap, rhs * chunk)) return rc;
+    if (kind == GETRF || kind == GESV || kind == GETRS)
+      if (int rc = grow(reinterpret_cast<void**>(&s.piv), &s.pcap, size_t(n) * chunk * sizeof(int))) return rc;
+    if (info)
+      if (int rc = grow(reinterpret_cast<void**>(&s.info), &s.icap, size_t(chunk) * sizeof(int))) return rc;
+  }
+  const bool writes_a = (kind == POTRF || kind == GETRF || kind == POSV || kind == GESV);
+  const bool writes_piv = (kind == GETRF || kind == GESV);
+  const bool writes_info = info && writes_a;
+  int c = 0;
+  for (int64_t m = 0; m < batch; m += chunk, ++c) {
+    Slot& s = ctx.slot[c % kSlots];
+    const int64_t cnt = std::min(chunk, batch - m);
+    T* dA = static_cast<T*>(s.a);
+    T* dB = static_cast<T*>(s.b);
+    TSDX_CK(cudaMemcpyAsync(dA, reinterpret_cast<const char*>(A) + m * mat, mat * cnt, cudaMemcpyHostToDevice, s.st), "H2D A");
+    if (has_b && nrhs > 0)
+      TSDX_CK(cudaMemcpyAsync(dB, reinterpret_cast<const char*>(B) + m * rhs, rhs * cnt, cudaMemcpyHostToDevice, s.st), "H2D B");
+    if (kind == GETRS)
+      TSDX_CK(cudaMemcpyAsync(s.piv, piv_in + m * n, size_t(n) * cnt * sizeof(int), cudaMemcpyHostToDevice, s.st), "H2D piv");
+    const int rc = run_device<T>(kind, dA, s.piv, n, cnt, dB, nrhs, s.piv, writes_info ? s.info : nullptr, s.st);
+    if (rc) return rc;
+    if (writes_a)
+      TSDX_CK(cudaMemcpyAsync(reinterpret_cast<char*>(A) + m * mat, dA, mat * cnt, cudaMemcpyDeviceToHost, s.st), "D2H A");
+    if (has_b && nrhs > 0)
+      TSDX_CK(cudaMemcpyAsync(reinterpret_cast<char*>(B) + m * rhs, dB, rhs * cnt, cudaMemcpyDeviceToHost, s.st), "D2H B");
+    if (writes_piv)
+      TSDX_CK(cudaMemcpyAsync(piv + m * n, s.piv, size_t(n) * cnt * sizeof(int), cudaMemcpyDeviceToHost, s.st), "D2H piv");
+    if (writes_info)
+      TSDX_CK(cudaMemcpyAsync(info + m, s.info, size_t(cnt) * sizeof(int), cudaMemcpyDeviceToHost, s.st), "D2H info");
+  }
+  for (auto& s : ctx.slot) TSDX_CK(cudaStreamSynchronize(s.st), "cudaStreamSynchronize");
+  return TSDX_OK;
+}
+
+}  // namespace
+}  // namespace host
+}  // namespace tsdx
+
+using tsdx::host::GESV;
+using tsdx::host::GETRF;
+using tsdx::host::GETRS;
+using tsdx::host::POSV;
+using tsdx::host::POTRF;
+using tsdx::host::POTRS;
+using tsdx::host::run_device;
+using tsdx::host::run_host;
+
+#define API extern "C" __attribute__((visibility("default")))
+#define ST(s) static_cast<cudaStream_t>(s)
+
+API int tsdx_cuda_available(void) {
+  int c = 0;
+  return cudaGetDeviceCount(&c) == cudaSuccess && c > 0 ? 1 : 0;
+}
+API const char* tsdx_cuda_last_error(void) { return tsdx::host::g_err.c_str(); }
+API int64_t tsdx_cuda_launch_count(void) { return tsdx::host::launch_counter().load(); }
+
+#define TSDX_DEFINE(T, S)                                                                                      \
+  API int tsdx_cuda_potrf_##S(T* A, int n, int64_t batch, int* info, void* st) {                               \
+    return run_device<T>(POTRF, A, nullptr, n, batch, nullptr, 0, nullptr, info, ST(st));                      \
+  }                                                                                                            \
+  API int tsdx_cuda_getrf_##S(T* A, int n, int64_t batch, int* piv, int* info, void* st) {                     \
+    return run_device<T>(GETRF, A, nullptr, n, batch, nullptr, 0, piv, info, ST(st));                          \
+  }                                                                                                            \
+  API int tsdx_cuda_potrs_##S(const T* L, int n, int64_t batch, T* B, int nrhs, void* st) {                    \
+    return run_device<T>(POTRS, const_cast<T*>(L), nullptr, n, batch, B, nrhs, nullptr, nullptr, ST(st));      \
+  }                                                                                                            \
+  API int tsdx_cuda_getrs_##S(const T* LU, const int* piv, int n, int64_t batch, T* B, int nrhs, void* st) {   \
+    return run_device<T>(GETRS, const_cast<T*>(LU), piv, n, batch, B, nrhs, nullptr, nullptr, ST(st));         \
+  }                                                                                                            \
+  API int tsdx_cuda_posv_##S(T* A, int n, int64_t batch, T* B, int nrhs, int* info, void* st) {                \
+    return run_device<T>(POSV, A, nullptr, n, batch, B, nrhs, nullptr, info, ST(st));                          \
+  }                                                                                                            \
+  API int tsdx_cuda_gesv_##S(T* A, int n, int64_t batch, T* B, int nrhs, int* piv, int* info, void* st) {      \
+    return run_device<T>(GESV, A, nullptr, n, batch, B, nrhs, piv, info, ST(st));                              \
+  }                                                                                                            \
+  API int tsdx_cuda_cholesky_batched_host_##S(T* A, int n, int64_t batch, int* info) {                         \
+    return run_host<T>(POTRF, A, nullptr, n, batch, nullptr, 0, nullptr, info);                                \
+  }                                                                                                            \
+  API int tsdx_cuda_lu_batched_host_##S(T* A, int n, int64_t batch, int* piv, int* info) {                     \
+    return run_host<T>(GETRF, A, nullptr, n, batch, nullptr, 0, piv, info);                                    \
+  }                                                                                                            \
+  API int tsdx_cuda_cholesky_solve_batched_host_##S(const T* L, int n, int64_t batch, T* B, int nrhs) {        \
+    return run_host<T>(POTRS, const_cast<T*>(L), nullptr, n, batch, B, nrhs, nullptr, nullptr);                \
+  }                                                                                                            \
+  API int tsdx_cuda_lu_solve_batched_host_##S(const T* LU, const int* piv, int n, int64_t batch, T* B,         \
+                                               int nrhs) {                                                     \
+    return run_host<T>(GETRS, const_cast<T*>(LU), piv, n, batch, B, nrhs, nullptr, nullptr);                   \
+  }                                                                                                            \
+  API int tsdx_cuda_posv_batched_host_##S(T* A, int n, int64_t batch, T* B, int nrhs, int* info) {             \
+    return run_host<T>(POSV, A, nullptr, n, batch, B, nrhs, nullptr, info);                                    \
+  }                                                                                                            \
+  API int tsdx_cuda_gesv_batched_host_##S(T* A, int n, int64_t batch, T* B, int nrhs, int* piv, int* info) {   \
+    return run_host<T>(GESV, A, nullptr, n, batch, B, nrhs, piv, info);                                        \
+  }
+
+TSDX_DEFINE(float, f32)
+TSDX_DEFINE(double, f64)

@@ -1,0 +1,150 @@
+// Host-side launchers: map a runtime (n, nrhs) onto a compiled (NP, NRHS, TW)
+// team kernel and size a persistent grid from the occupancy of that kernel.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <string>
+
+#include "chol_team.cuh"
+#include "lu_team.cuh"
+#include "solve.cuh"
+
+namespace tsdx {
+namespace host {
+
+using dev::FastDiv;
+using dev::SolveArgs;
+
+// Errors of the CUDA runtime, per calling thread.
+void set_cuda_error(cudaError_t e, const char* what);
+std::atomic<long long>& launch_counter();
+
+int device_sms(int dev);
+
+// Compiled padded sizes; a matrix of order n runs in the smallest NP >= n
+// (identity padding is exactly transparent to every result, see team.cuh).
+inline int np_of(int n) {
+  return n <= 4 ? 4 : n <= 8 ? 8 : n <= 16 ? 16 : n <= 24 ? 24 : n <= 32 ? 32 : n <= 40 ? 40 : n <= 48 ? 48 : n <= 56 ? 56 : 64;
+}
+// Right-hand sides are solved in passes of at most 8 columns.
+inline int nrhs_bucket(int r) { return r == 0 ? 0 : r == 1 ? 1 : r <= 4 ? 4 : 8; }
+template <class T> constexpr int tw_for(int np) { return np <= 32 ? 1 : 2; }
+
+// Widest cp.async chunk that keeps every row start aligned.
+template <class T> inline int vec_for(const void* p, int n) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  const int row = n * int(sizeof(T));
+  if (row % 16 == 0 && a % 16 == 0) return 16;
+  if (row % 8 == 0 && a % 8 == 0) return 8;
+  return 4;
+}
+
+template <class Kern>
+int grid_for(Kern kern, int smem, long long ctas_needed) {
+  int devi = 0;
+  cudaGetDevice(&devi);
+  static thread_local int last_dev = -1;
+  (void)last_dev;
+  int occ = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 128, smem);
+  if (e != cudaSuccess || occ < 1) occ = 1;
+  const long long cap = (long long)device_sms(devi) * occ;
+  return (int)(ctas_needed < cap ? (ctas_needed < 1 ? 1 : ctas_needed) : cap);
+}
+
+template <class Kern>
+int prepare(Kern kern, int smem) {
+  // the attribute is per function and per device; setting it is idempotent
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) { set_cuda_error(e, "cudaFuncSetAttribute"); return -5; }
+  }
+  return 0;
+}
+
+template <class T, int NP, int NRHS, bool CHOL>
+int launch_team(const SolveArgs<T>& a, int vec, cudaStream_t st) {
+  constexpr int TW = tw_for<T>(NP);
+  using L = dev::Layout<T, NP, NRHS, TW>;
+  constexpr int SMEM = CHOL ? dev::CholSmem<T, NP, NRHS, TW>::CTA : dev::LuSmem<T, NP, NRHS, TW>::CTA;
+  auto kern = CHOL ? dev::chol_team_kernel<T, NP, NRHS, TW> : dev::lu_team_kernel<T, NP, NRHS, TW>;
+  if (int rc = prepare(kern, SMEM)) return rc;
+  const long long units = (a.batch + L::S - 1) / L::S;
+  const long long ctas = (units + (4 / TW) - 1) / (4 / TW);
+  const int grid = grid_for(kern, SMEM, ctas);
+  kern<<<grid, 128, SMEM, st>>>(a, FastDiv((unsigned)a.n), vec);
+  launch_counter().fetch_add(1);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) { set_cuda_error(e, "kernel launch"); return -5; }
+  return 0;
+}
+
+template <class T, int NP, int NRHS, bool LU>
+int launch_trs(const SolveArgs<T>& a, int vec, cudaStream_t st) {
+  constexpr int SMEM = dev::SolveSmem<T, NP>::CTA;
+  auto kern = dev::trs_kernel<T, NP, NRHS, LU>;
+  if (int rc = prepare(kern, SMEM)) return rc;
+  const long long ctas = (a.batch + 3) / 4;
+  const int grid = grid_for(kern, SMEM, ctas);
+  kern<<<grid, 128, SMEM, st>>>(a, FastDiv((unsigned)a.n), vec);
+  launch_counter().fetch_add(1);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) { set_cuda_error(e, "kernel launch"); return -5; }
+  return 0;
+}
+
+#define TSDX_NP_SWITCH(NPV, BODY)                 \
+  switch (NPV) {                                  \
+    case 4: { constexpr int NP_ = 4; BODY; }      \
+    case 8: { constexpr int NP_ = 8; BODY; }      \
+    case 16: { constexpr int NP_ = 16; BODY; }    \
+    case 24: { constexpr int NP_ = 24; BODY; }    \
+    case 32: { constexpr int NP_ = 32; BODY; }    \
+    case 40: { constexpr int NP_ = 40; BODY; }    \
+    case 48: { constexpr int NP_ = 48; BODY; }    \
+    case 56: { constexpr int NP_ = 56; BODY; }    \
+    default: { constexpr int NP_ = 64; BODY; }    \
+  }
+#define TSDX_RHS_SWITCH(RV, BODY)                 \
+  switch (RV) {                                   \
+    case 0: { constexpr int R_ = 0; BODY; }       \
+    case 1: { constexpr int R_ = 1; BODY; }       \
+    case 4: { constexpr int R_ = 4; BODY; }       \
+    default: { constexpr int R_ = 8; BODY; }      \
+  }
+
+// One fused pass: factor A (and solve B columns [b0, b0 + nrhs), nrhs <= 8).
+template <class T, bool CHOL>
+int run_team(const SolveArgs<T>& a, cudaStream_t st) {
+  const int vec = vec_for<T>(a.A, a.n);
+  SolveArgs<T> b = a;
+  b.rowdiv = FastDiv((unsigned)(a.n * int(sizeof(T)) / vec));
+  const int np = np_of(a.n), rb = nrhs_bucket(a.nrhs);
+  TSDX_NP_SWITCH(np, TSDX_RHS_SWITCH(rb, return (launch_team<T, NP_, R_, CHOL>(b, vec, st))));
+  return 0;
+}
+
+// One solve pass from a factor (nrhs <= 8).
+template <class T, bool LU>
+int run_trs(const SolveArgs<T>& a, cudaStream_t st) {
+  const int vec = vec_for<T>(a.A, a.n);
+  SolveArgs<T> b = a;
+  b.rowdiv = FastDiv((unsigned)(a.n * int(sizeof(T)) / vec));
+  const int np = np_of(a.n) <= 32 ? 32 : 64, rb = nrhs_bucket(a.nrhs);
+  if (np == 32) {
+    TSDX_RHS_SWITCH(rb == 0 ? 1 : rb, return (launch_trs<T, 32, (R_ > 0 ? R_ : 1), LU>(b, vec, st)));
+  }
+  TSDX_RHS_SWITCH(rb == 0 ? 1 : rb, return (launch_trs<T, 64, (R_ > 0 ? R_ : 1), LU>(b, vec, st)));
+  return 0;
+}
+
+// Explicitly instantiated in the per-type translation units.
+template <class T> int run_lu(const SolveArgs<T>& a, cudaStream_t st);
+template <class T> int run_chol(const SolveArgs<T>& a, cudaStream_t st);
+template <class T> int run_getrs(const SolveArgs<T>& a, cudaStream_t st);
+template <class T> int run_potrs(const SolveArgs<T>& a, cudaStream_t st);
+
+}  // namespace host
+}  // namespace tsdx

@@ -1,0 +1,179 @@
+// Register-resident "team" kernels for batched small-matrix Cholesky / LU on sm_100a.
+//
+// One team of TW warps owns one matrix (TW == 1 and n <= 16: one warp owns 32/G
+// matrices, G lanes each). Lane l of a team owns matrix rows {l + G*s}; with
+// TW > 1 the columns are dealt to the warps in groups of 16 bytes. The whole
+// matrix plus its right-hand sides (the augmented columns NP..NP+NRHS-1) lives in
+// registers for the entire factorization, so the rank-1 trailing update never
+// touches shared memory; shared memory only carries the per-step broadcasts (the
+// pivot row, the Cholesky column, the multipliers when TW > 1) and the coalesced
+// staging of the global loads and stores.
+//
+// Bit-exactness. Each element receives exactly the reference's chain of
+// operations (TinySolverDx kernels.hpp): LU (kernels.hpp:91-119) a_ij <-
+// fma(-l_ik, u_kj, a_ij) in increasing k with l_ik = a_ik / u_kk an IEEE
+// division; Cholesky as the reference's default simd backend compiles it
+// (kernels.hpp:57-87: fused for n <= 16, separately rounded product and
+// subtraction for n >= 17). The forward substitution is fused into the
+// elimination as extra columns, which is the same chain as kernels.hpp:184-193 /
+// 214-218. Pivoting is implicit: rows never move, a position table replays the
+// reference's row swaps so its tie-breaking (strict '>', first maximum wins, NaN
+// never wins unless it sits on the diagonal position) is reproduced exactly, and
+// each row is written out at the position where it was retired, which is exactly
+// where the reference's full-row swaps leave it.
+//
+// The back substitution is column-oriented (decreasing k), so X agrees with the
+// reference to rounding (backward error within c*n*u), not bit-for-bit.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tsdx {
+namespace dev {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+template <class T> struct KeyT;
+template <> struct KeyT<double> { using U = unsigned long long; };
+template <> struct KeyT<float> { using U = unsigned; };
+
+__device__ __forceinline__ unsigned long long key_bits(double v) { return (unsigned long long)__double_as_longlong(fabs(v)); }
+__device__ __forceinline__ unsigned key_bits(float v) { return __float_as_uint(fabsf(v)); }
+
+__device__ __forceinline__ double fma_(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fma_(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+// s - x*y with the product rounded first (never contracted)
+__device__ __forceinline__ double sub_mul(double s, double x, double y) { return __dsub_rn(s, __dmul_rn(x, y)); }
+__device__ __forceinline__ float sub_mul(float s, float x, float y) { return __fsub_rn(s, __fmul_rn(x, y)); }
+__device__ __forceinline__ double div_(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float div_(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double sqrt_(double a) { return __dsqrt_rn(a); }
+__device__ __forceinline__ float sqrt_(float a) { return __fsqrt_rn(a); }
+
+__device__ __forceinline__ void named_barrier(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// ---- argmax over a lane segment: larger key wins, ties go to the smaller position.
+__device__ __forceinline__ int seg_argmax(unsigned mask, unsigned long long key, int pos, unsigned long long* kout) {
+  const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+  const unsigned mhi = __reduce_max_sync(mask, hi);
+  const unsigned mlo = __reduce_max_sync(mask, hi == mhi ? lo : 0u);
+  const int cand = (hi == mhi && lo == mlo) ? pos : 0x7fffffff;
+  *kout = ((unsigned long long)mhi << 32) | mlo;
+  return __reduce_min_sync(mask, cand);
+}
+__device__ __forceinline__ int seg_argmax(unsigned mask, unsigned key, int pos, unsigned* kout) {
+  const unsigned mk = __reduce_max_sync(mask, key);
+  *kout = mk;
+  return __reduce_min_sync(mask, key == mk ? pos : 0x7fffffff);
+}
+
+// ---- cp.async (LDGSTS) staging of a global byte range into padded rows --------
+template <int VEC>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if constexpr (VEC == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+  else if constexpr (VEC == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Fast division of small non-negative ints by a runtime divisor d (d <= 4096,
+// x < 2^19): q = umulhi(x, ceil(2^32/d)) is exact in that range.
+struct FastDiv {
+  unsigned d, m;
+  __host__ __device__ FastDiv() : d(1), m(0) {}
+  __host__ __device__ explicit FastDiv(unsigned dd) : d(dd), m((unsigned)((0x100000000ull + dd - 1) / dd)) {}
+  __device__ __forceinline__ unsigned div(unsigned x) const { return d == 1 ? x : __umulhi(x, m); }
+};
+
+// ---- layout -------------------------------------------------------------------
+template <class T, int NP, int NRHS, int TW>
+struct Layout {
+  static constexpr int G = (TW > 1 || NP > 16) ? 32 : NP <= 4 ? 4 : NP <= 8 ? 8 : 16;  // lanes per matrix
+  static constexpr int S = (TW == 1) ? 32 / G : 1;                                        // matrices per warp
+  static constexpr int MR = (NP + G - 1) / G;                                             // row slots per lane
+  static constexpr int NC = NP + NRHS;                                                    // augmented columns
+  static constexpr int CW = (TW == 1) ? 1 : int(16 / sizeof(T));                         // column group width
+  static constexpr int NGRP = (NC + CW - 1) / CW;
+  static constexpr int MC = (TW == 1) ? NC : ((NGRP + TW - 1) / TW) * CW;                 // column slots per warp
+  static constexpr int RS = NP * int(sizeof(T)) + 16;                                     // padded staging row (bytes)
+  static constexpr int BUF = NP * RS;                                                     // staging bytes per matrix
+  static_assert(NP % 4 == 0, "NP must be a multiple of 4");
+  static_assert(TW == 1 || (NP / CW) % TW == 0, "B columns must start a column group");
+  static_assert(MR <= 2, "at most two row slots per lane");
+  __host__ __device__ static constexpr int col(int w, int c) {
+    return TW == 1 ? c : ((c / CW) * TW + w) * CW + (c % CW);
+  }
+  __host__ __device__ static constexpr int cmin(int c) { return col(0, c); }
+  __host__ __device__ static constexpr int cmax(int c) { return col(TW - 1, c); }
+  __host__ __device__ static constexpr int owner(int j) { return TW == 1 ? 0 : (j / CW) % TW; }
+  __host__ __device__ static constexpr int slot(int j) { return TW == 1 ? j : ((j / CW) / TW) * CW + (j % CW); }
+};
+
+template <class T>
+struct SolveArgs {
+  T* A;            // (batch, n, n) row-major; overwritten by the factor
+  T* B;            // (batch, n, ldb) row-major; columns [b0, b0 + nrhs) are solved in place
+  int* piv;        // (batch, n) LU pivots, 0-based sequential (LU only)
+  int* info;       // (batch) or nullptr
+  long long batch;
+  int n, ldb, b0, nrhs;
+  FastDiv rowdiv;  // divides by the number of copy chunks per row
+};
+
+}  // namespace dev
+}  // namespace tsdx
+
+namespace tsdx {
+namespace dev {
+
+// 16-byte shared-memory vector access (2 doubles / 4 floats).
+template <class T> struct Vec16;
+template <> struct Vec16<double> {
+  using type = double2;
+  static constexpr int n = 2;
+  __device__ static __forceinline__ double get(const double2& v, int i) { return i == 0 ? v.x : v.y; }
+  __device__ static __forceinline__ void set(double2& v, int i, double x) { if (i == 0) v.x = x; else v.y = x; }
+};
+template <> struct Vec16<float> {
+  using type = float4;
+  static constexpr int n = 4;
+  __device__ static __forceinline__ float get(const float4& v, int i) { return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w; }
+  __device__ static __forceinline__ void set(float4& v, int i, float x) {
+    if (i == 0) v.x = x; else if (i == 1) v.y = x; else if (i == 2) v.z = x; else v.w = x;
+  }
+};
+
+// Copies rows [0, rows) of a dense (rows x n) stack at g into padded staging rows
+// (row stride RS bytes) with VEC-byte cp.async chunks; rc = n*sizeof(T)/VEC.
+template <class T, int VEC, int RS, int BUF>
+__device__ __forceinline__ void stage_in(unsigned char* stage, const char* g, int rows, int n, int rc,
+                                         const FastDiv& rowdiv, const FastDiv& ndiv, int tt, int TT) {
+  const int chunks = rows * rc;
+  for (int e = tt; e < chunks; e += TT) {
+    const int row = (int)rowdiv.div(e), ch = e - row * rc;
+    const int mm = (int)ndiv.div(row), r = row - mm * n;
+    cp_async<VEC>(stage + mm * BUF + r * RS + ch * VEC, g + (long long)row * n * int(sizeof(T)) + ch * VEC);
+  }
+  cp_async_commit();
+}
+template <class T, int VEC, int RS, int BUF>
+__device__ __forceinline__ void stage_out(const unsigned char* stage, char* g, int rows, int n, int rc,
+                                          const FastDiv& rowdiv, const FastDiv& ndiv, int tt, int TT) {
+  const int chunks = rows * rc;
+  for (int e = tt; e < chunks; e += TT) {
+    const int row = (int)rowdiv.div(e), ch = e - row * rc;
+    const int mm = (int)ndiv.div(row), r = row - mm * n;
+    const unsigned char* src = stage + mm * BUF + r * RS + ch * VEC;
+    char* dst = g + (long long)row * n * int(sizeof(T)) + ch * VEC;
+    if constexpr (VEC == 16) *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(src);
+    else if constexpr (VEC == 8) *reinterpret_cast<uint2*>(dst) = *reinterpret_cast<const uint2*>(src);
+    else *reinterpret_cast<unsigned*>(dst) = *reinterpret_cast<const unsigned*>(src);
+  }
+}
+
+}  // namespace dev
+}  // namespace tsdx
