@@ -16,7 +16,9 @@ template <class T, int NP, int NRHS, int TW>
 struct LuSmem {
   using L = Layout<T, NP, NRHS, TW>;
   static constexpr int STAGE = L::S * L::BUF;
-  static constexpr int UROW = TW * L::S * L::MC * int(sizeof(T));
+  // per-warp pivot-row buffer, padded so every segment's buffer is 16-byte aligned
+  static constexpr int MCP = (L::MC * int(sizeof(T)) + 15) / 16 * 16 / int(sizeof(T));
+  static constexpr int UROW = TW * L::S * MCP * int(sizeof(T));
   static constexpr int MULT = (TW > 1) ? 2 * NP * int(sizeof(T)) + 32 : 0;
   static constexpr int TEAM = ((STAGE + UROW + MULT) + 127) / 128 * 128;
   static constexpr int CTA = TEAM * (4 / TW);
@@ -43,7 +45,7 @@ __global__ void __launch_bounds__(128) lu_team_kernel(SolveArgs<T> p, FastDiv nd
   const int segbase = seg * G;
   const unsigned segmask = (G == 32) ? kFull : (((1u << G) - 1u) << segbase);
   unsigned char* stage = smem + team * SM::TEAM;
-  T* urow = reinterpret_cast<T*>(stage + SM::STAGE) + (w * S + seg) * MC;
+  T* urow = reinterpret_cast<T*>(stage + SM::STAGE) + (w * S + seg) * SM::MCP;
   T* mult = reinterpret_cast<T*>(stage + SM::STAGE + SM::UROW);                       // [2][NP]
   int* sinfo = reinterpret_cast<int*>(stage + SM::STAGE + SM::UROW + 2 * NP * int(sizeof(T)));  // [2][4]
 

@@ -45,7 +45,8 @@ __global__ void __launch_bounds__(128) trs_kernel(SolveArgs<T> p, FastDiv ndiv, 
       __syncwarp();
       if (lane == 0)
         for (int k = 0; k < n; ++k) {  // kernels.hpp:207-213: swaps applied in k order
-          const int q = p.piv[m * n + k];
+          int q = p.piv[m * n + k];
+          q = (q < 0 || q >= n) ? k : q;  // out-of-range pivots are ignored, never dereferenced
           const int t = perm[k]; perm[k] = perm[q]; perm[q] = t;
         }
     }
