@@ -13,25 +13,25 @@
 namespace tsdx {
 namespace dev {
 
-template <class T, int NP, int NRHS, int TW>
+template <class T, int NP, int NRHS, int TW, int WPC>
 struct CholSmem {
   using L = Layout<T, NP, NRHS, TW>;
   static constexpr int STAGE = L::S * L::BUF;
   static constexpr int COL = ((TW > 1) ? 2 : L::S) * NP * int(sizeof(T));
   static constexpr int INFO = (TW > 1) ? 2 * 16 : 0;
   static constexpr int TEAM = ((STAGE + COL + INFO) + 127) / 128 * 128;
-  static constexpr int CTA = TEAM * (4 / TW);
+  static constexpr int CTA = TEAM * (WPC / TW);
 };
 
-template <class T, int NP, int NRHS, int TW>
-__global__ void __launch_bounds__(128) chol_team_kernel(SolveArgs<T> p, FastDiv ndiv, int vec) {
+template <class T, int NP, int NRHS, int TW, int WPC>
+__global__ void __launch_bounds__(WPC * 32, 1) chol_team_kernel(SolveArgs<T> p, FastDiv ndiv, int vec) {
   using L = Layout<T, NP, NRHS, TW>;
-  using SM = CholSmem<T, NP, NRHS, TW>;
+  using SM = CholSmem<T, NP, NRHS, TW, WPC>;
   using V = Vec16<T>;
   using VT = typename V::type;
   constexpr int G = L::G, S = L::S, MR = L::MR, MC = L::MC;
   constexpr int VN = V::n;
-  constexpr int TPC = 4 / TW, TT = TW * 32;
+  constexpr int TPC = WPC / TW, TT = TW * 32;
   constexpr int NA = (TW == 1) ? NP : NP / TW;
   constexpr bool FUSED = NP <= 16;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -53,9 +53,12 @@ __global__ void __launch_bounds__(128) chol_team_kernel(SolveArgs<T> p, FastDiv 
   const int n = p.n;
   const long long nn = (long long)n * n;
   const int rc = n * int(sizeof(T)) / vec;
-  const long long nteams = (long long)gridDim.x * TPC;
+  const long long per_round = (long long)gridDim.x * TPC * S;
 
-  for (long long m0 = ((long long)blockIdx.x * TPC + team) * S; m0 < p.batch; m0 += nteams * S) {
+  for (long long base = (long long)blockIdx.x * TPC * S; base < p.batch; base += per_round) {
+    __syncthreads();  // keep the CTA's warps on the same stretch of code
+    const long long m0 = base + (long long)team * S;
+    if (m0 >= p.batch) continue;
     const int cnt = (int)min((long long)S, p.batch - m0);
     if (vec == 16) stage_in<T, 16, L::RS, L::BUF>(stage, reinterpret_cast<const char*>(p.A + m0 * nn), cnt * n, n, rc, p.rowdiv, ndiv, tt, TT);
     else if (vec == 8) stage_in<T, 8, L::RS, L::BUF>(stage, reinterpret_cast<const char*>(p.A + m0 * nn), cnt * n, n, rc, p.rowdiv, ndiv, tt, TT);
@@ -114,13 +117,14 @@ __global__ void __launch_bounds__(128) chol_team_kernel(SolveArgs<T> p, FastDiv 
         const T d = __shfl_sync(kFull, a[ds][CK], dl);
         bad = !(d > T(0));
         lkk = sqrt_(bad ? T(1) : d);
+        const T ry = rcp_(lkk);
 #pragma unroll
         for (int s = 0; s < MR; ++s) {
           const int r = lsl + G * s;
-          const T l = div_(a[s][CK], lkk);
           const bool below = r > k && r < NP;
-          lcol[s] = below ? l : T(0);
-          a[s][CK] = below ? l : (r == k ? lkk : a[s][CK]);
+          lcol[s] = T(0);
+          if (below) lcol[s] = div_by(a[s][CK], lkk, ry);
+          a[s][CK] = below ? lcol[s] : (r == k ? lkk : a[s][CK]);
           if (r < NP) cb[r] = lcol[s];
         }
         if constexpr (TW > 1) {
@@ -163,7 +167,7 @@ __global__ void __launch_bounds__(128) chol_team_kernel(SolveArgs<T> p, FastDiv 
       }
       // forward substitution on the right-hand sides this warp owns
       if constexpr (NRHS > 0) {
-        const T rk = div_(T(1), lkk);
+        const T rk = rcp_(lkk);
         if (lsl == (k % G)) dinv[ds] = rk;
 #pragma unroll
         for (int c = NA; c < MC; ++c) {

@@ -6,13 +6,18 @@
 // index of the first exactly-zero pivot, after which that column is skipped and
 // the factorization completes; A is overwritten by the packed L\U factors and B
 // by the solution.
+//
+// Execution: one persistent CTA of WPC warps per SM slot; every round each team
+// of the CTA takes the next matrix and the whole CTA walks the fully unrolled
+// code together (a __syncthreads per round), so the instruction stream fetched
+// for one warp serves all of them.
 #pragma once
 #include "team.cuh"
 
 namespace tsdx {
 namespace dev {
 
-template <class T, int NP, int NRHS, int TW>
+template <class T, int NP, int NRHS, int TW, int WPC>
 struct LuSmem {
   using L = Layout<T, NP, NRHS, TW>;
   static constexpr int STAGE = L::S * L::BUF;
@@ -21,19 +26,19 @@ struct LuSmem {
   static constexpr int UROW = TW * L::S * MCP * int(sizeof(T));
   static constexpr int MULT = (TW > 1) ? 2 * NP * int(sizeof(T)) + 32 : 0;
   static constexpr int TEAM = ((STAGE + UROW + MULT) + 127) / 128 * 128;
-  static constexpr int CTA = TEAM * (4 / TW);
+  static constexpr int CTA = TEAM * (WPC / TW);
 };
 
-template <class T, int NP, int NRHS, int TW>
-__global__ void __launch_bounds__(128) lu_team_kernel(SolveArgs<T> p, FastDiv ndiv, int vec) {
+template <class T, int NP, int NRHS, int TW, int WPC>
+__global__ void __launch_bounds__(WPC * 32, 1) lu_team_kernel(SolveArgs<T> p, FastDiv ndiv, int vec) {
   using L = Layout<T, NP, NRHS, TW>;
-  using SM = LuSmem<T, NP, NRHS, TW>;
+  using SM = LuSmem<T, NP, NRHS, TW, WPC>;
   using K = typename KeyT<T>::U;
   using V = Vec16<T>;
   using VT = typename V::type;
   constexpr int G = L::G, S = L::S, MR = L::MR, MC = L::MC;
   constexpr int VN = V::n;
-  constexpr int TPC = 4 / TW;                      // teams per CTA (128 threads)
+  constexpr int TPC = WPC / TW;                    // teams per CTA
   constexpr int TT = TW * 32;                      // threads per team
   constexpr int NA = (TW == 1) ? NP : NP / TW;     // A-column slots per warp (B slots follow)
   extern __shared__ __align__(128) unsigned char smem[];
@@ -46,7 +51,7 @@ __global__ void __launch_bounds__(128) lu_team_kernel(SolveArgs<T> p, FastDiv nd
   const unsigned segmask = (G == 32) ? kFull : (((1u << G) - 1u) << segbase);
   unsigned char* stage = smem + team * SM::TEAM;
   T* urow = reinterpret_cast<T*>(stage + SM::STAGE) + (w * S + seg) * SM::MCP;
-  T* mult = reinterpret_cast<T*>(stage + SM::STAGE + SM::UROW);                       // [2][NP]
+  T* mult = reinterpret_cast<T*>(stage + SM::STAGE + SM::UROW);                                 // [2][NP]
   int* sinfo = reinterpret_cast<int*>(stage + SM::STAGE + SM::UROW + 2 * NP * int(sizeof(T)));  // [2][4]
 
   auto team_sync = [&]() {
@@ -57,9 +62,12 @@ __global__ void __launch_bounds__(128) lu_team_kernel(SolveArgs<T> p, FastDiv nd
   const int n = p.n;
   const long long nn = (long long)n * n;
   const int rc = n * int(sizeof(T)) / vec;
-  const long long nteams = (long long)gridDim.x * TPC;
+  const long long per_round = (long long)gridDim.x * TPC * S;
 
-  for (long long m0 = ((long long)blockIdx.x * TPC + team) * S; m0 < p.batch; m0 += nteams * S) {
+  for (long long base = (long long)blockIdx.x * TPC * S; base < p.batch; base += per_round) {
+    __syncthreads();  // keep the CTA's warps on the same stretch of code
+    const long long m0 = base + (long long)team * S;
+    if (m0 >= p.batch) continue;
     const int cnt = (int)min((long long)S, p.batch - m0);
     {
       const char* g = reinterpret_cast<const char*>(p.A + m0 * nn);
@@ -135,7 +143,7 @@ __global__ void __launch_bounds__(128) lu_team_kernel(SolveArgs<T> p, FastDiv nd
 #pragma unroll
         for (int s = 0; s < MR; ++s) {
           const T v = a[s][CK];
-          K key = isnan(v) ? (pos[s] == k ? ~K(0) : K(0)) : key_bits(v) + 1;
+          const K key = isnan(v) ? (pos[s] == k ? ~K(0) : K(0)) : key_bits(v) + 1;
           const bool better = act[s] && (key > bk || (key == bk && pos[s] < bp));
           bk = better ? key : bk;
           bp = better ? pos[s] : bp;
@@ -148,16 +156,18 @@ __global__ void __launch_bounds__(128) lu_team_kernel(SolveArgs<T> p, FastDiv nd
         for (int s = 0; s < MR; ++s) myslot = (act[s] && pos[s] == bpos) ? s : myslot;
         const unsigned bal = __ballot_sync(kFull, myslot >= 0);
         wl = segbase + __ffs((bal & segmask) >> segbase) - 1;
-        wslot = __shfl_sync(kFull, myslot, wl);
+        if (MR > 1) wslot = __shfl_sync(kFull, myslot, wl);
         T mine = a[0][CK];
         if (MR > 1) mine = (myslot == MR - 1) ? a[MR - 1][CK] : mine;
         vpk = __shfl_sync(kFull, mine, wl);
+        const T ry = rcp_(vpk);
 #pragma unroll
         for (int s = 0; s < MR; ++s) {
           const bool doit = act[s] && (myslot != s) && !zero;
-          const T l = div_(a[s][CK], vpk);
-          mlt[s] = doit ? l : T(0);
-          a[s][CK] = doit ? l : a[s][CK];
+          if (doit) {
+            mlt[s] = div_by(a[s][CK], vpk, ry);
+            a[s][CK] = mlt[s];
+          }
         }
         if constexpr (TW > 1) {
           T* mb = mult + (k & 1) * NP;
@@ -197,38 +207,47 @@ __global__ void __launch_bounds__(128) lu_team_kernel(SolveArgs<T> p, FastDiv nd
       if (lane == wl) {
 #pragma unroll
         for (int s = 0; s < MR; ++s) {
-          if (s != wslot) continue;
+          if (MR > 1 && s != wslot) continue;
 #pragma unroll
-          for (int c = 0; c < MC; ++c)
-            if (L::cmax(c) > k) urow[c] = a[s][c];
+          for (int c0 = 0; c0 < MC; c0 += VN) {
+            if (L::cmax(c0 + VN - 1 < MC ? c0 + VN - 1 : MC - 1) <= k) continue;
+            if (c0 + VN <= MC) {
+              VT v;
+#pragma unroll
+              for (int q = 0; q < VN; ++q) V::set(v, q, a[s][c0 + q]);
+              *reinterpret_cast<VT*>(urow + c0) = v;
+            } else {
+#pragma unroll
+              for (int q = 0; q < VN; ++q)
+                if (c0 + q < MC) urow[c0 + q] = a[s][c0 + q];
+            }
+          }
         }
       }
       __syncwarp();
-      T u[MC];
-#pragma unroll
-      for (int c = 0; c < MC; ++c) u[c] = T(0);
+      // rank-1 update of the active rows (the right-hand sides ride along as columns)
 #pragma unroll
       for (int c0 = 0; c0 < MC; c0 += VN) {
-        if (L::cmax(c0 + VN - 1) <= k) continue;
+        if (L::cmax(c0 + VN - 1 < MC ? c0 + VN - 1 : MC - 1) <= k) continue;
+        T u[VN];
         if (c0 + VN <= MC) {
           const VT v = *reinterpret_cast<const VT*>(urow + c0);
 #pragma unroll
-          for (int q = 0; q < VN; ++q) u[c0 + q] = V::get(v, q);
+          for (int q = 0; q < VN; ++q) u[q] = V::get(v, q);
         } else {
 #pragma unroll
-          for (int q = 0; q < VN; ++q)
-            if (c0 + q < MC) u[c0 + q] = urow[c0 + q];
+          for (int q = 0; q < VN; ++q) u[q] = (c0 + q < MC) ? urow[c0 + q] : T(0);
         }
-      }
-      // rank-1 update of the active rows (the right-hand sides ride along as columns)
 #pragma unroll
-      for (int s = 0; s < MR; ++s) {
-        const bool rowon = act[s] && !zero;
+        for (int s = 0; s < MR; ++s) {
+          const bool rowon = act[s] && !zero;
 #pragma unroll
-        for (int c = 0; c < MC; ++c) {
-          if (L::cmax(c) <= k) continue;
-          const bool colon = (L::cmin(c) > k) || (L::col(w, c) > k);
-          if (rowon && colon) a[s][c] = fma_(-mlt[s], u[c], a[s][c]);
+          for (int q = 0; q < VN; ++q) {
+            const int c = c0 + q;
+            if (c >= MC || L::cmax(c) <= k) continue;
+            const bool colon = (L::cmin(c) > k) || (L::col(w, c) > k);
+            if (rowon && colon) a[s][c] = fma_(-mlt[s], u[q], a[s][c]);
+          }
         }
       }
     }
@@ -264,7 +283,7 @@ __global__ void __launch_bounds__(128) lu_team_kernel(SolveArgs<T> p, FastDiv nd
       if constexpr (TW == 1) {
         T dinv[MR];
 #pragma unroll
-        for (int s = 0; s < MR; ++s) dinv[s] = div_(T(1), diag[s]);
+        for (int s = 0; s < MR; ++s) dinv[s] = rcp_(diag[s]);
 #pragma unroll
         for (int k = NP - 1; k >= 0; --k) {
           int own = -1;
@@ -319,7 +338,7 @@ __global__ void __launch_bounds__(128) lu_team_kernel(SolveArgs<T> p, FastDiv nd
           const unsigned bal = __ballot_sync(kFull, own >= 0);
           const int ol = __ffs(bal) - 1;
           const T ukk = *reinterpret_cast<const T*>(stage + k * L::RS + k * int(sizeof(T)));
-          const T rinv = div_(T(1), ukk);
+          const T rinv = rcp_(ukk);
           T x[NB];
 #pragma unroll
           for (int c = 0; c < NB; ++c) {

@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(128) trs_kernel(SolveArgs<T> p, FastDiv ndiv, 
     // backward: U x = y (LU) or L^T x = y (Cholesky)
     for (int k = n - 1; k >= 0; --k) {
       const int ks = k >> 5, kl = k & 31;
-      const T rinv = div_(T(1), at(k, k));
+      const T rinv = rcp_(at(k, k));
       T ck[MR];
 #pragma unroll
       for (int s = 0; s < MR; ++s) {
