@@ -269,3 +269,29 @@ def test_argument_errors():
     with pytest.raises(ValueError):
         capi.check(capi.call("tsdx_cuda_getrf_f64", capi.ptr(a), 3, 2, None, None, capi.stream_ptr()))
     assert capi.call("tsdx_cuda_potrf_f64", capi.ptr(a), 3, 0, None, capi.stream_ptr()) == 0
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_markstein_division(dtype):
+    """div_by (shared reciprocal + Markstein correction, team.cuh) equals IEEE division bit for bit."""
+    rng = np.random.default_rng(17)
+    m = 4_000_000
+    lo, hi = (-300, 300) if dtype == np.float64 else (-35, 35)
+    a = (rng.standard_normal(m) * 10.0 ** rng.uniform(lo, hi, m)).astype(dtype)
+    b = (rng.standard_normal(m) * 10.0 ** rng.uniform(lo, hi, m)).astype(dtype)
+    fi = np.finfo(dtype)
+    edge = np.array([0.0, -0.0, np.inf, -np.inf, np.nan, fi.tiny, fi.tiny / 4, fi.max, -fi.max, 1.0, -1.0,
+                     2.0, 0.5, 3.0, 1.0 - fi.eps / 2, 1.0 + fi.eps, fi.smallest_subnormal], dtype)
+    ea, eb = np.meshgrid(edge, edge)
+    ones = np.full(m // 4, 1.0, dtype) + rng.integers(0, 1 << 20, m // 4).astype(dtype) * fi.eps  # near-1 divisors
+    a = np.concatenate([a, ea.ravel(), rng.standard_normal(m // 4).astype(dtype)])
+    b = np.concatenate([b, eb.ravel(), ones])
+    ta, tb = dev(a), dev(b)
+    fast, ieee = torch.empty_like(ta), torch.empty_like(ta)
+    name = "tsdx_internal_div_check_" + capi.sfx(np.dtype(dtype))
+    capi.check(getattr(capi.lib(), name)(capi.ptr(ta), capi.ptr(tb), capi.ptr(fast), capi.ptr(ieee), a.size,
+                                        capi.stream_ptr()))
+    f, e = host(fast), host(ieee)
+    iv = np.uint64 if dtype == np.float64 else np.uint32
+    same = (f.view(iv) == e.view(iv)) | (np.isnan(f) & np.isnan(e))
+    assert same.all(), (a[~same][:5], b[~same][:5])

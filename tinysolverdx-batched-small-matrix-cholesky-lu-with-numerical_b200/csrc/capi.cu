@@ -217,6 +217,36 @@ API int tsdx_cuda_available(void) {
 API const char* tsdx_cuda_last_error(void) { return tsdx::host::g_err.c_str(); }
 API int64_t tsdx_cuda_launch_count(void) { return tsdx::host::launch_counter().load(); }
 
+// Self-check of the Markstein-corrected division used by the kernels (team.cuh
+// div_by) against the IEEE division, element by element. Not part of the solver
+// API; the test-suite calls it on adversarial operand sets.
+namespace {
+template <class T>
+__global__ void div_check_kernel(const T* a, const T* b, T* fast, T* ieee, long long count) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const T y = tsdx::dev::rcp_(b[i]);
+  fast[i] = tsdx::dev::div_by(a[i], b[i], y);
+  ieee[i] = tsdx::dev::div_(a[i], b[i]);
+}
+template <class T>
+int div_check(const T* a, const T* b, T* fast, T* ieee, int64_t count, void* st) {
+  if (count <= 0) return TSDX_OK;
+  div_check_kernel<T><<<(unsigned)((count + 255) / 256), 256, 0, ST(st)>>>(a, b, fast, ieee, count);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) { tsdx::host::set_cuda_error(e, "kernel launch"); return TSDX_ERR_CUDA; }
+  return TSDX_OK;
+}
+}  // namespace
+API int tsdx_internal_div_check_f64(const double* a, const double* b, double* fast, double* ieee, int64_t count,
+                                     void* st) {
+  return div_check<double>(a, b, fast, ieee, count, st);
+}
+API int tsdx_internal_div_check_f32(const float* a, const float* b, float* fast, float* ieee, int64_t count,
+                                     void* st) {
+  return div_check<float>(a, b, fast, ieee, count, st);
+}
+
 #define TSDX_DEFINE(T, S)                                                                                      \
   API int tsdx_cuda_potrf_##S(T* A, int n, int64_t batch, int* info, void* st) {                               \
     return run_device<T>(POTRF, A, nullptr, n, batch, nullptr, 0, nullptr, info, ST(st));                      \

@@ -1,5 +1,5 @@
-// Host-side launchers: map a runtime (n, nrhs) onto a compiled (NP, NRHS, TW)
-// team kernel and size a persistent grid from the occupancy of that kernel.
+// Host-side launchers: map a runtime (n, nrhs) onto a compiled (NP, NRHS) kernel
+// and size a persistent grid from the occupancy of that kernel.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -7,9 +7,8 @@
 #include <cstdint>
 #include <string>
 
-#include "chol_team.cuh"
+#include "chol_blk.cuh"
 #include "lu_blk.cuh"
-#include "lu_team.cuh"
 #include "solve.cuh"
 
 namespace tsdx {
@@ -31,12 +30,6 @@ inline int np_of(int n) {
 }
 // Right-hand sides are solved in passes of at most 8 columns.
 inline int nrhs_bucket(int r) { return r == 0 ? 0 : r == 1 ? 1 : r <= 4 ? 4 : 8; }
-template <class T> constexpr int tw_for(int np) { return np <= 32 ? 1 : 2; }
-// Warps per persistent CTA: as many as the register file holds for the layout.
-template <class T> constexpr int wpc_for(int np) {
-  return np <= 16 ? 16 : np <= 32 ? (sizeof(T) == 8 ? 12 : 16) : 8;
-}
-
 // Widest cp.async chunk that keeps every row start aligned.
 template <class T> inline int vec_for(const void* p, int n) {
   const uintptr_t a = reinterpret_cast<uintptr_t>(p);
@@ -69,33 +62,15 @@ int prepare(Kern kern, int smem) {
   return 0;
 }
 
+// Blocked one-warp-per-matrix LU / Cholesky (lu_blk.cuh, chol_blk.cuh): a
+// persistent CTA per SM with as many warps as shared memory holds (at most 16).
 template <class T, int NP, int NRHS, bool CHOL>
-int launch_team(const SolveArgs<T>& a, int vec, cudaStream_t st) {
-  constexpr int TW = tw_for<T>(NP);
-  constexpr int WPC = wpc_for<T>(NP);
-  using L = dev::Layout<T, NP, NRHS, TW>;
-  constexpr int SMEM = CHOL ? dev::CholSmem<T, NP, NRHS, TW, WPC>::CTA : dev::LuSmem<T, NP, NRHS, TW, WPC>::CTA;
-  static_assert(SMEM <= 227 * 1024, "shared memory per CTA");
-  auto kern = CHOL ? dev::chol_team_kernel<T, NP, NRHS, TW, WPC> : dev::lu_team_kernel<T, NP, NRHS, TW, WPC>;
-  if (int rc = prepare(kern, SMEM)) return rc;
-  const long long units = (a.batch + L::S - 1) / L::S;
-  const long long ctas = (units + (WPC / TW) - 1) / (WPC / TW);
-  const int grid = grid_for(kern, SMEM, ctas, WPC * 32);
-  kern<<<grid, WPC * 32, SMEM, st>>>(a, FastDiv((unsigned)a.n), vec);
-  launch_counter().fetch_add(1);
-  const cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) { set_cuda_error(e, "kernel launch"); return -5; }
-  return 0;
-}
-
-// Blocked one-warp-per-matrix LU (lu_blk.cuh): as many warps per CTA as shared memory holds.
-template <class T, int NP, int NRHS>
-int launch_lu_blk(const SolveArgs<T>& a, int vec, cudaStream_t st) {
+int launch_blk(const SolveArgs<T>& a, int vec, cudaStream_t st) {
   using C = dev::BlkCfg<T, NP, NRHS>;
   constexpr int FIT = (227 * 1024) / C::WARPB;
   constexpr int WPC = FIT < 1 ? 1 : (FIT > 16 ? 16 : FIT);
   constexpr int SMEM = WPC * C::WARPB;
-  auto kern = dev::lu_blk_kernel<T, NP, NRHS, WPC>;
+  auto kern = CHOL ? dev::chol_blk_kernel<T, NP, NRHS, WPC> : dev::lu_blk_kernel<T, NP, NRHS, WPC>;
   if (int rc = prepare(kern, SMEM)) return rc;
   const long long units = (a.batch + C::S - 1) / C::S;
   const long long ctas = (units + WPC - 1) / WPC;
@@ -148,11 +123,7 @@ int run_team(const SolveArgs<T>& a, cudaStream_t st) {
   SolveArgs<T> b = a;
   b.rowdiv = FastDiv((unsigned)(a.n * int(sizeof(T)) / vec));
   const int np = np_of(a.n), rb = nrhs_bucket(a.nrhs);
-  if constexpr (!CHOL) {
-    TSDX_NP_SWITCH(np, TSDX_RHS_SWITCH(rb, return (launch_lu_blk<T, NP_, R_>(b, vec, st))));
-  } else {
-    TSDX_NP_SWITCH(np, TSDX_RHS_SWITCH(rb, return (launch_team<T, NP_, R_, CHOL>(b, vec, st))));
-  }
+  TSDX_NP_SWITCH(np, TSDX_RHS_SWITCH(rb, return (launch_blk<T, NP_, R_, CHOL>(b, vec, st))));
   return 0;
 }
 
