@@ -89,6 +89,27 @@ int tsdx_cuda_posv_batched_host_f64(double* A, int n, int64_t batch, double* B, 
 int tsdx_cuda_gesv_batched_host_f32(float* A, int n, int64_t batch, float* B, int nrhs, int* piv, int* info);
 int tsdx_cuda_gesv_batched_host_f64(double* A, int n, int64_t batch, double* B, int nrhs, int* piv, int* info);
 
+/* ---- mixed precision + iterative refinement (no reference counterpart) -------------
+ * Solves A x = b (one right-hand side, A (batch, n, n) float64, NOT modified, B (batch, n)
+ * float64 overwritten by x) by factoring a power-of-two scaled copy of A in low precision
+ * and refining with float64 residuals until the normwise backward error
+ * ||b - A x|| / (||A||_F ||x|| + ||b||) (runtime.cpp:230-242) is <= tol or itmax
+ * corrections have been applied. Matrices that do not converge are re-solved by the
+ * plain float64 kernel in the same call, so every returned x is either refined or fp64.
+ *   tier   (batch) int8 per matrix, or NULL to use default_tier for all:
+ *          0 fp16 (scaled, tensor cores), 1 bf16 (tensor cores), 2 fp32, 3 fp64 directly
+ *   info   (batch) or NULL: fp64 info for fallback matrices, low-precision info otherwise
+ *   status (batch) or NULL: refinement steps used (>= 0), or -1 = solved by the fp64 fallback
+ *   bwd    (batch) or NULL: the last backward error measured by the refinement
+ * gesv_ir pivots (LU); posv_ir assumes A symmetric positive definite (Cholesky).
+ */
+int tsdx_cuda_gesv_ir_f64(const double* A, int n, int64_t batch, double* B, const signed char* tier,
+                          int default_tier, int itmax, double tol, int* info, int* status, double* bwd,
+                          void* stream);
+int tsdx_cuda_posv_ir_f64(const double* A, int n, int64_t batch, double* B, const signed char* tier,
+                          int default_tier, int itmax, double tol, int* info, int* status, double* bwd,
+                          void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -41,7 +41,9 @@ for _s in ("f32", "f64"):
     })
 SIGNATURES.update({"tsdx_cuda_available": [], "tsdx_cuda_launch_count": [],
                    "tsdx_internal_div_check_f64": [_P, _P, _P, _P, _I64, _P],
-                   "tsdx_internal_div_check_f32": [_P, _P, _P, _P, _I64, _P]})
+                   "tsdx_internal_div_check_f32": [_P, _P, _P, _P, _I64, _P],
+                   "tsdx_cuda_gesv_ir_f64": [_P, _I, _I64, _P, _P, _I, _I, C.c_double, _P, _P, _P, _P],
+                   "tsdx_cuda_posv_ir_f64": [_P, _I, _I64, _P, _P, _I, _I, C.c_double, _P, _P, _P, _P]})
 
 _lib = None
 

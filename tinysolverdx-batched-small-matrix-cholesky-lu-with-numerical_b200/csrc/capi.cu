@@ -22,6 +22,9 @@
 namespace tsdx {
 namespace host {
 
+int run_ir(bool spd, const double* A, int n, long long batch, double* B, const signed char* tier, int default_tier,
+           int itmax, double tol, int* info, int* status, double* bwd, cudaStream_t st);
+
 namespace {
 thread_local std::string g_err;
 std::atomic<long long> g_launches{0};
@@ -76,6 +79,8 @@ int run_device(Kind kind, T* A, const int* piv_in, int n, int64_t batch, T* B, i
   a.batch = batch;
   a.n = n;
   a.ldb = nrhs;
+  a.status = nullptr;
+  a.wf = 1;
   if (kind == POTRF || kind == GETRF || kind == POSV || kind == GESV) {
     a.b0 = 0;
     a.nrhs = std::min(nrhs, 8);
@@ -245,6 +250,42 @@ API int tsdx_internal_div_check_f64(const double* a, const double* b, double* fa
 API int tsdx_internal_div_check_f32(const float* a, const float* b, float* fast, float* ieee, int64_t count,
                                      void* st) {
   return div_check<float>(a, b, fast, ieee, count, st);
+}
+
+// ---- mixed precision + iterative refinement ------------------------------------
+namespace {
+int ir_entry(bool spd, const double* A, int n, int64_t batch, double* B, const signed char* tier, int default_tier,
+             int itmax, double tol, int* info, int* status, double* bwd, void* st) {
+  if (n < 1 || n > 64) return TSDX_ERR_N;
+  if (batch < 0) return TSDX_ERR_BATCH;
+  if (!A || !B) return TSDX_ERR_NULL;
+  if (default_tier < 0 || default_tier > 3 || itmax < 0 || !(tol > 0.0)) return TSDX_ERR_NRHS;
+  if (batch == 0) return TSDX_OK;
+  cudaStream_t s = ST(st);
+  int* stat = status;
+  if (!stat) {
+    // the fallback pass needs the per-matrix status; stream-ordered scratch when the caller has none
+    const cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&stat), size_t(batch) * sizeof(int), s);
+    if (e != cudaSuccess) { tsdx::host::set_cuda_error(e, "cudaMallocAsync"); return TSDX_ERR_CUDA; }
+  }
+  int rc = tsdx::host::run_ir(spd, A, n, batch, B, tier, default_tier, itmax, tol, info, stat, bwd, s);
+  if (!status) {
+    const cudaError_t e = cudaFreeAsync(stat, s);
+    if (e != cudaSuccess && rc == 0) { tsdx::host::set_cuda_error(e, "cudaFreeAsync"); rc = TSDX_ERR_CUDA; }
+  }
+  return rc;
+}
+}  // namespace
+
+API int tsdx_cuda_gesv_ir_f64(const double* A, int n, int64_t batch, double* B, const signed char* tier,
+                              int default_tier, int itmax, double tol, int* info, int* status, double* bwd,
+                              void* stream) {
+  return ir_entry(false, A, n, batch, B, tier, default_tier, itmax, tol, info, status, bwd, stream);
+}
+API int tsdx_cuda_posv_ir_f64(const double* A, int n, int64_t batch, double* B, const signed char* tier,
+                              int default_tier, int itmax, double tol, int* info, int* status, double* bwd,
+                              void* stream) {
+  return ir_entry(true, A, n, batch, B, tier, default_tier, itmax, tol, info, status, bwd, stream);
 }
 
 #define TSDX_DEFINE(T, S)                                                                                      \

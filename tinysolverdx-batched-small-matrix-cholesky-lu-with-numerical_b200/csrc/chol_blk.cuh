@@ -49,7 +49,8 @@ __global__ void __launch_bounds__(WPC * 32, 1) chol_blk_kernel(SolveArgs<T> p, F
     const long long m0 = base + (long long)warp * S;
     if (m0 >= p.batch) continue;
     const int cnt = (int)min((long long)S, p.batch - m0);
-    const bool live = seg < cnt;
+    const bool live = seg < cnt && !(p.status && p.status[m0 + seg] >= 0);
+    if (!__any_sync(kFull, live)) continue;
     {
       const char* g = reinterpret_cast<const char*>(p.A + m0 * nn);
       if (vec == 16) stage_in<T, 16, RS, C::SEGB>(wbase, g, cnt * n, n, rc, p.rowdiv, ndiv, lane, 32);
@@ -264,6 +265,7 @@ __global__ void __launch_bounds__(WPC * 32, 1) chol_blk_kernel(SolveArgs<T> p, F
     if (live && lsl == 0 && p.info) p.info[m0 + seg] = info;
     // zero the upper triangle, then copy out
     __syncwarp();
+    if (!p.wf) continue;
 #pragma unroll
     for (int s = 0; s < MR; ++s) {
       const int r = lsl + G * s;
@@ -271,11 +273,19 @@ __global__ void __launch_bounds__(WPC * 32, 1) chol_blk_kernel(SolveArgs<T> p, F
       for (int c = r + 1; c < n; ++c) at(r, c) = T(0);
     }
     __syncwarp();
-    {
+    if (!p.status) {
       char* g = reinterpret_cast<char*>(p.A + m0 * nn);
       if (vec == 16) stage_out<T, 16, RS, C::SEGB>(wbase, g, cnt * n, n, rc, p.rowdiv, ndiv, lane, 32);
       else if (vec == 8) stage_out<T, 8, RS, C::SEGB>(wbase, g, cnt * n, n, rc, p.rowdiv, ndiv, lane, 32);
       else stage_out<T, 4, RS, C::SEGB>(wbase, g, cnt * n, n, rc, p.rowdiv, ndiv, lane, 32);
+    } else {
+      for (int mm = 0; mm < cnt; ++mm) {
+        if (p.status[m0 + mm] >= 0) continue;
+        char* g = reinterpret_cast<char*>(p.A + (m0 + mm) * nn);
+        if (vec == 16) stage_out<T, 16, RS, C::SEGB>(wbase + mm * C::SEGB, g, n, n, rc, p.rowdiv, ndiv, lane, 32);
+        else if (vec == 8) stage_out<T, 8, RS, C::SEGB>(wbase + mm * C::SEGB, g, n, n, rc, p.rowdiv, ndiv, lane, 32);
+        else stage_out<T, 4, RS, C::SEGB>(wbase + mm * C::SEGB, g, n, n, rc, p.rowdiv, ndiv, lane, 32);
+      }
     }
     __syncwarp();
   }

@@ -76,7 +76,8 @@ __global__ void __launch_bounds__(WPC * 32, 1) lu_blk_kernel(SolveArgs<T> p, Fas
     const long long m0 = base + (long long)warp * S;
     if (m0 >= p.batch) continue;
     const int cnt = (int)min((long long)S, p.batch - m0);
-    const bool live = seg < cnt;
+    const bool live = seg < cnt && !(p.status && p.status[m0 + seg] >= 0);
+    if (!__any_sync(kFull, live)) continue;
     {
       const char* g = reinterpret_cast<const char*>(p.A + m0 * nn);
       if (vec == 16) stage_in<T, 16, RS, C::SEGB>(wbase, g, cnt * n, n, rc, p.rowdiv, ndiv, lane, 32);
@@ -305,20 +306,23 @@ __global__ void __launch_bounds__(WPC * 32, 1) lu_blk_kernel(SolveArgs<T> p, Fas
     }
     // ------------------------------------------------------ piv, info, L\U
     if (live) {
+      if (p.wf) {
 #pragma unroll
-      for (int t = 0; t < MR; ++t) {
-        const int k = lsl + G * t;
-        if (k < n) p.piv[(m0 + seg) * n + k] = pvs[k];
+        for (int t = 0; t < MR; ++t) {
+          const int k = lsl + G * t;
+          if (k < n) p.piv[(m0 + seg) * n + k] = pvs[k];
+        }
       }
       if (lsl == 0 && p.info) p.info[m0 + seg] = info;
     }
     __syncwarp();
-    {
+    if (p.wf) {
       char* g = reinterpret_cast<char*>(p.A + m0 * nn);
       const int chunks = cnt * n * rc;
       for (int e = lane; e < chunks; e += 32) {
         const int row = (int)p.rowdiv.div(e), ch = e - row * rc;
         const int mm = (int)ndiv.div(row), r = row - mm * n;
+        if (p.status && p.status[m0 + mm] >= 0) continue;
         const unsigned char* mseg = wbase + mm * C::SEGB;
         const int src = reinterpret_cast<const int*>(mseg + C::MAT)[r];
         const unsigned char* sp = mseg + src * RS + ch * vec;

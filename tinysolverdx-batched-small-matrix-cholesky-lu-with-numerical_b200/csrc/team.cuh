@@ -150,7 +150,9 @@ struct SolveArgs {
   int* info;       // (batch) or nullptr
   long long batch;
   int n, ldb, b0, nrhs;
-  FastDiv rowdiv;  // divides by the number of copy chunks per row
+  FastDiv rowdiv;      // divides by the number of copy chunks per row
+  const int* status;   // optional: matrices with status[m] >= 0 are skipped (no reads, no writes)
+  int wf;              // 1: A <- factor and piv written (reference semantics); 0: A left untouched
 };
 
 }  // namespace dev
