@@ -89,6 +89,14 @@ int tsdx_cuda_posv_batched_host_f64(double* A, int n, int64_t batch, double* B, 
 int tsdx_cuda_gesv_batched_host_f32(float* A, int n, int64_t batch, float* B, int nrhs, int* piv, int* info);
 int tsdx_cuda_gesv_batched_host_f64(double* A, int n, int64_t batch, double* B, int nrhs, int* piv, int* info);
 
+/* One-shot solves that return only (x, info), like the reference's Python-level
+ * tsdx.gesv / tsdx.posv (python/tinysolverdx/__init__.py:102-111): A is read and left
+ * untouched, B is overwritten by X, no factor or pivots travel back to the host. */
+int tsdx_cuda_gesv_solve_host_f32(const float* A, int n, int64_t batch, float* B, int nrhs, int* info);
+int tsdx_cuda_gesv_solve_host_f64(const double* A, int n, int64_t batch, double* B, int nrhs, int* info);
+int tsdx_cuda_posv_solve_host_f32(const float* A, int n, int64_t batch, float* B, int nrhs, int* info);
+int tsdx_cuda_posv_solve_host_f64(const double* A, int n, int64_t batch, double* B, int nrhs, int* info);
+
 /* ---- mixed precision + iterative refinement (no reference counterpart) -------------
  * Solves A x = b (one right-hand side, A (batch, n, n) float64, NOT modified, B (batch, n)
  * float64 overwritten by x) by factoring a power-of-two scaled copy of A in low precision

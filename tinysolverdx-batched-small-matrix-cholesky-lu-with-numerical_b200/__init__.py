@@ -1,1 +1,183 @@
-"""B200-native batched small-matrix Cholesky / LU (placeholder, filled in below)."""
+"""B200-native batched small-matrix Cholesky / LU — a drop-in for TinySolverDx.
+
+The NumPy-facing functions mirror TinySolverDx ``python/tinysolverdx/__init__.py``
+(same names, arguments, dtype rules, return values and exceptions): inputs are
+(batch, n, n) arrays (a single (n, n) matrix is also accepted) with n in 1..64;
+float32 -> fp32, float64 -> fp64, float16 -> emulated fp16. ``backend="cuda"``
+runs on the B200 for every function, the solves included; the CPU backends
+("auto", "naive", "scalar", "simd") reproduce the reference's results bit for bit.
+
+Beyond the reference:
+  * ``gesv_ir`` / ``posv_ir``: mixed-precision factorization (fp16/bf16 tensor
+    cores or fp32) with fp64 iterative refinement and an fp64 fallback;
+  * ``solve_stream``: one call over an uneven stream of matrices (n 2..64, Cholesky
+    and LU mixed, 1..8 right-hand sides);
+  * ``selector``: the learned per-matrix precision-tier selector;
+  * ``device``: the same solvers on torch CUDA tensors, stream-ordered, no copies.
+"""
+import numpy as np
+
+from . import _core
+from ._core import has_cuda, has_openmp, num_threads, set_num_threads, unit_roundoff  # noqa: F401
+from ._core import (chol_backward_error, lu_backward_error, solve_backward_error,  # noqa: F401
+                    solve_forward_error, reference_solve)
+
+__all__ = ["cholesky", "lu", "cholesky_solve", "lu_solve", "posv", "gesv", "round_to",
+           "has_cuda", "has_openmp", "num_threads", "set_num_threads", "unit_roundoff",
+           "chol_backward_error", "lu_backward_error", "solve_backward_error",
+           "solve_forward_error", "reference_solve", "gesv_ir", "posv_ir"]
+
+_DEFAULT_PREC = {np.dtype(np.float32): "fp32", np.dtype(np.float64): "fp64", np.dtype(np.float16): "fp16"}
+
+
+def _fn(name, arr):
+    # one core entry point per storage dtype (no implicit casting)
+    return getattr(_core, f"{name}_{'f64' if arr.dtype == np.float64 else 'f32'}")
+
+
+def _prep(a, precision, ndim_single):
+    a = np.asarray(a)
+    single = a.ndim == ndim_single
+    if single:
+        a = a[None]
+    out_dtype = a.dtype
+    if precision is None:
+        if a.dtype not in _DEFAULT_PREC:
+            raise TypeError(f"unsupported dtype {a.dtype}; use float16/32/64")
+        precision = _DEFAULT_PREC[a.dtype]
+    if precision not in ("fp16", "bf16", "fp32", "fp64"):
+        raise ValueError("precision must be one of fp16, bf16, fp32, fp64")
+    work = np.float64 if (precision == "fp64" and a.dtype == np.float64) else np.float32
+    if a.dtype == np.float64 and precision != "fp64":
+        work = np.float64  # keep wide storage; the core rounds into the target format
+    return np.ascontiguousarray(a, dtype=work), precision, single, out_dtype
+
+
+def _finish(x, out_dtype, precision):
+    if precision == "fp16" and out_dtype == np.float16:
+        return x.astype(np.float16)
+    return x
+
+
+def cholesky(A, precision=None, backend="auto"):
+    """Lower Cholesky factors and LAPACK-style info (0 = ok, k>0: pivot k not positive)."""
+    a, p, single, dt = _prep(A, precision, 2)
+    L, info = _fn("cholesky", a)(a, p, backend)
+    L = _finish(L, dt, p)
+    return (L[0], info[0]) if single else (L, info)
+
+
+def lu(A, precision=None, backend="auto"):
+    """Packed LU with partial pivoting: (LU, piv, info). piv is scipy/LAPACK style (0-based)."""
+    a, p, single, dt = _prep(A, precision, 2)
+    LU, piv, info = _fn("lu", a)(a, p, backend)
+    LU = _finish(LU, dt, p)
+    return (LU[0], piv[0], info[0]) if single else (LU, piv, info)
+
+
+def _rhs(B, ref, single):
+    B = np.asarray(B)
+    if single:
+        B = B[:, None] if B.ndim == 1 else B
+        B = B[None]
+    elif B.ndim == 2:
+        B = B[:, :, None]
+    return np.ascontiguousarray(B, dtype=ref.dtype)
+
+
+def cholesky_solve(L, B, precision=None, backend="auto"):
+    """Solve L L^T x = B given factors from :func:`cholesky`."""
+    l, p, single, dt = _prep(np.asarray(L), precision, 2)
+    vec = np.asarray(B).ndim == (1 if single else 2)
+    X = _fn("cholesky_solve", l)(l, _rhs(B, l, single), p, backend)
+    X = _finish(X, dt, p)
+    X = X[..., 0] if vec else X
+    return X[0] if single else X
+
+
+def lu_solve(LU, piv, B, precision=None, backend="auto"):
+    """Solve A x = B given (LU, piv) from :func:`lu`."""
+    l, p, single, dt = _prep(LU, precision, 2)
+    pv = np.ascontiguousarray(np.asarray(piv)[None] if single else piv, dtype=np.int32)
+    vec = np.asarray(B).ndim == (1 if single else 2)
+    X = _fn("lu_solve", l)(l, pv, _rhs(B, l, single), p, backend)
+    X = _finish(X, dt, p)
+    X = X[..., 0] if vec else X
+    return X[0] if single else X
+
+
+def _fused(kind, A, B, precision):
+    a, p, single, dt = _prep(A, precision, 2)
+    if p not in ("fp32", "fp64") or (p == "fp64") != (a.dtype == np.float64):
+        return None
+    vec = np.asarray(B).ndim == (1 if single else 2)
+    X, info = _fn(f"{kind}_cuda", a)(a, _rhs(B, a, single))
+    X = X[..., 0] if vec else X
+    return (X[0], info[0]) if single else (X, info)
+
+
+def posv(A, B, precision=None, backend="auto"):
+    """Solve SPD systems A x = B. Returns (x, info)."""
+    if backend == "cuda":
+        r = _fused("posv", A, B, precision)
+        if r is not None:
+            return r
+    L, info = cholesky(A, precision, backend)
+    return cholesky_solve(L, B, precision, backend), info
+
+
+def gesv(A, B, precision=None, backend="auto"):
+    """Solve general systems A x = B with partial pivoting. Returns (x, info)."""
+    if backend == "cuda":
+        r = _fused("gesv", A, B, precision)
+        if r is not None:
+            return r
+    LU, piv, info = lu(A, precision, backend)
+    return lu_solve(LU, piv, B, precision, backend), info
+
+
+def round_to(x, precision):
+    """Round values to the nearest number representable in ``precision`` (float64 in/out)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    return _core.round_to_f64(x, precision)
+
+
+# ---- mixed precision + iterative refinement ------------------------------------------
+TIERS = {"fp16": 0, "bf16": 1, "fp32": 2, "fp64": 3}
+
+
+def _ir(spd, A, b, tier, itmax, tol):
+    import torch
+    from . import device
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    single = A.ndim == 2
+    if single:
+        A, b = A[None], b[None]
+    if A.ndim != 3 or A.shape[1] != A.shape[2] or b.shape != A.shape[:2]:
+        raise ValueError("expected A (batch, n, n) and b (batch, n)")
+    a = torch.from_numpy(A).cuda()
+    x = torch.from_numpy(b).cuda()
+    t = None
+    default = 2
+    if isinstance(tier, str):
+        default = TIERS[tier]
+    elif tier is not None:
+        t = torch.as_tensor(np.asarray(tier, dtype=np.int8)).cuda()
+    info, status, bwd = device.ir(a, x, spd, tier=t, default_tier=default, itmax=itmax, tol=tol)
+    out = (x.cpu().numpy(), info.cpu().numpy(), status.cpu().numpy(), bwd.cpu().numpy())
+    return tuple(o[0] for o in out) if single else out
+
+
+def gesv_ir(A, b, tier="fp32", itmax=3, tol=1e-15):
+    """Mixed-precision LU + fp64 iterative refinement (float64 A, one right-hand side).
+
+    ``tier`` is "fp16", "bf16", "fp32", "fp64" or a per-matrix int8 array (0..3).
+    Returns (x, info, status, bwd): status >= 0 is the number of refinement steps,
+    -1 means the matrix was re-solved by the plain fp64 path."""
+    return _ir(False, A, b, tier, itmax, tol)
+
+
+def posv_ir(A, b, tier="fp32", itmax=3, tol=1e-15):
+    """Mixed-precision Cholesky + fp64 iterative refinement (SPD float64 A)."""
+    return _ir(True, A, b, tier, itmax, tol)

@@ -71,11 +71,11 @@ def build_core(force=False):
         return None
     suffix = sysconfig.get_config_var("EXT_SUFFIX")
     out = PKG / ("_core" + suffix)
-    deps = [src, CSRC / "host_api.hpp", ROOT / "include" / "tsdx_cuda.h", LIB]
+    deps = [src, CSRC / "host_api.hpp", ROOT / "include" / "tsdx_cuda.h", LIB, pathlib.Path(__file__)]
     if not force and out.exists() and out.stat().st_mtime >= max(d.stat().st_mtime for d in deps if d.exists()):
         return out
     cxx = "/usr/bin/g++"
-    cmd = [cxx, "-O2", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden",
+    cmd = [cxx, "-O3", "-march=x86-64-v3", "-ffp-contract=off", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden",
            "-I" + pybind11.get_include(), "-I" + sysconfig.get_paths()["include"],
            "-I" + str(CSRC), "-I" + str(ROOT / "include"),
            str(src), "-o", str(out), "-L" + str(OUT), "-ltsdx_cuda", "-Wl,-rpath,$ORIGIN/_lib"]

@@ -38,6 +38,8 @@ for _s in ("f32", "f64"):
         f"tsdx_cuda_lu_solve_batched_host_{_s}": [_P, _P, _I, _I64, _P, _I],
         f"tsdx_cuda_posv_batched_host_{_s}": [_P, _I, _I64, _P, _I, _P],
         f"tsdx_cuda_gesv_batched_host_{_s}": [_P, _I, _I64, _P, _I, _P, _P],
+        f"tsdx_cuda_gesv_solve_host_{_s}": [_P, _I, _I64, _P, _I, _P],
+        f"tsdx_cuda_posv_solve_host_{_s}": [_P, _I, _I64, _P, _I, _P],
     })
 SIGNATURES.update({"tsdx_cuda_available": [], "tsdx_cuda_launch_count": [],
                    "tsdx_internal_div_check_f64": [_P, _P, _P, _P, _I64, _P],

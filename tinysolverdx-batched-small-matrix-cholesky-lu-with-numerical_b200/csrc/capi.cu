@@ -139,13 +139,16 @@ int grow(void** p, size_t* cap, size_t need) {
     if (e_ != cudaSuccess) { set_cuda_error(e_, what); return TSDX_ERR_CUDA; } \
   } while (0)
 
+// keep_a: the one-shot solve leaves the caller's A untouched and returns no pivots
+// (the reference's Python-level gesv/posv return only (x, info), __init__.py:102-111).
 template <class T>
-int run_host(Kind kind, T* A, const int* piv_in, int n, int64_t batch, T* B, int nrhs, int* piv, int* info) {
+int run_host(Kind kind, T* A, const int* piv_in, int n, int64_t batch, T* B, int nrhs, int* piv, int* info,
+             bool keep_a = false) {
   if (int rc = check_common(n, batch, nrhs)) return rc;
   const bool has_b = (kind == POTRS || kind == GETRS || kind == POSV || kind == GESV);
   if (!has_b) nrhs = 0;
   if (!A) return TSDX_ERR_NULL;
-  if ((kind == GETRF || kind == GESV) && !piv) return TSDX_ERR_NULL;
+  if ((kind == GETRF || kind == GESV) && !piv && !keep_a) return TSDX_ERR_NULL;
   if (kind == GETRS && !piv_in) return TSDX_ERR_NULL;
   if (has_b && nrhs > 0 && !B) return TSDX_ERR_NULL;
   if (batch == 0) return TSDX_OK;
@@ -170,9 +173,9 @@ int run_host(Kind kind, T* A, const int* piv_in, int n, int64_t batch, T* B, int
     if (info)
       if (int rc = grow(reinterpret_cast<void**>(&s.info), &s.icap, size_t(chunk) * sizeof(int))) return rc;
   }
-  const bool writes_a = (kind == POTRF || kind == GETRF || kind == POSV || kind == GESV);
-  const bool writes_piv = (kind == GETRF || kind == GESV);
-  const bool writes_info = info && writes_a;
+  const bool writes_a = (kind == POTRF || kind == GETRF || kind == POSV || kind == GESV) && !keep_a;
+  const bool writes_piv = (kind == GETRF || kind == GESV) && !keep_a;
+  const bool writes_info = info && (kind == POTRF || kind == GETRF || kind == POSV || kind == GESV);
   int c = 0;
   for (int64_t m = 0; m < batch; m += chunk, ++c) {
     Slot& s = ctx.slot[c % kSlots];
@@ -184,6 +187,7 @@ int run_host(Kind kind, T* A, const int* piv_in, int n, int64_t batch, T* B, int
       TSDX_CK(cudaMemcpyAsync(dB, reinterpret_cast<const char*>(B) + m * rhs, rhs * cnt, cudaMemcpyHostToDevice, s.st), "H2D B");
     if (kind == GETRS)
       TSDX_CK(cudaMemcpyAsync(s.piv, piv_in + m * n, size_t(n) * cnt * sizeof(int), cudaMemcpyHostToDevice, s.st), "H2D piv");
+    // the device workspace copy of A may take the factor even when the caller's A is kept
     const int rc = run_device<T>(kind, dA, s.piv, n, cnt, dB, nrhs, s.piv, writes_info ? s.info : nullptr, s.st);
     if (rc) return rc;
     if (writes_a)
@@ -325,6 +329,12 @@ API int tsdx_cuda_posv_ir_f64(const double* A, int n, int64_t batch, double* B, 
   }                                                                                                            \
   API int tsdx_cuda_gesv_batched_host_##S(T* A, int n, int64_t batch, T* B, int nrhs, int* piv, int* info) {   \
     return run_host<T>(GESV, A, nullptr, n, batch, B, nrhs, piv, info);                                        \
+  }                                                                                                            \
+  API int tsdx_cuda_gesv_solve_host_##S(const T* A, int n, int64_t batch, T* B, int nrhs, int* info) {         \
+    return run_host<T>(GESV, const_cast<T*>(A), nullptr, n, batch, B, nrhs, nullptr, info, true);              \
+  }                                                                                                            \
+  API int tsdx_cuda_posv_solve_host_##S(const T* A, int n, int64_t batch, T* B, int nrhs, int* info) {         \
+    return run_host<T>(POSV, const_cast<T*>(A), nullptr, n, batch, B, nrhs, nullptr, info, true);              \
   }
 
 TSDX_DEFINE(float, f32)
