@@ -118,6 +118,30 @@ int tsdx_cuda_posv_ir_f64(const double* A, int n, int64_t batch, double* B, cons
                           int default_tier, int itmax, double tol, int* info, int* status, double* bwd,
                           void* stream);
 
+/* ---- uneven stream (no reference counterpart) -------------------------------------
+ * One call over `count` matrices of mixed order n in [1, 64], Cholesky (kind 0, posv)
+ * and LU (kind 1, gesv) mixed, 0..8 right-hand sides each, all in device memory:
+ *   A + aoff[i]  n_i x n_i row-major; overwritten by its factor when write_factors != 0
+ *   B + boff[i]  n_i x nrhs_i row-major right-hand sides, overwritten by X (B may be NULL)
+ *   piv + poff[i] n_i LU pivots (required when write_factors != 0)
+ *   info[i]      LAPACK-style info; -1 for an entry outside the supported sizes
+ * Factors, pivots, info and X are bit-identical to the dense tsdx_cuda_posv/gesv_*.
+ * The matrices are counting-sorted into buckets (kind, padded order, right-hand-side
+ * class) and drained by one persistent kernel through an atomic queue; the launches
+ * are stream-ordered and can be captured in a CUDA graph. sched: bit 0 / bit 1 run
+ * the n <= 8 / n <= 16 buckets one matrix per warp instead of packing 4 / 2 per warp
+ * (chosen by the autotuner of the Python layer). scratch: device memory of at least
+ * tsdx_cuda_stream_scratch_bytes(count) bytes, or NULL to allocate it on the stream. */
+int64_t tsdx_cuda_stream_scratch_bytes(int64_t count);
+int tsdx_cuda_solve_stream_f32(float* A, const int64_t* aoff, float* B, const int64_t* boff, int* piv,
+                               const int64_t* poff, int* info, const int* n, const int* nrhs,
+                               const signed char* kind, int64_t count, int write_factors, unsigned sched,
+                               void* scratch, int64_t scratch_bytes, void* stream);
+int tsdx_cuda_solve_stream_f64(double* A, const int64_t* aoff, double* B, const int64_t* boff, int* piv,
+                               const int64_t* poff, int* info, const int* n, const int* nrhs,
+                               const signed char* kind, int64_t count, int write_factors, unsigned sched,
+                               void* scratch, int64_t scratch_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -25,7 +25,7 @@ from ._core import (chol_backward_error, lu_backward_error, solve_backward_error
 __all__ = ["cholesky", "lu", "cholesky_solve", "lu_solve", "posv", "gesv", "round_to",
            "has_cuda", "has_openmp", "num_threads", "set_num_threads", "unit_roundoff",
            "chol_backward_error", "lu_backward_error", "solve_backward_error",
-           "solve_forward_error", "reference_solve", "gesv_ir", "posv_ir"]
+           "solve_forward_error", "reference_solve", "gesv_ir", "posv_ir", "solve_stream"]
 
 _DEFAULT_PREC = {np.dtype(np.float32): "fp32", np.dtype(np.float64): "fp64", np.dtype(np.float16): "fp16"}
 
@@ -181,3 +181,63 @@ def gesv_ir(A, b, tier="fp32", itmax=3, tol=1e-15):
 def posv_ir(A, b, tier="fp32", itmax=3, tol=1e-15):
     """Mixed-precision Cholesky + fp64 iterative refinement (SPD float64 A)."""
     return _ir(True, A, b, tier, itmax, tol)
+
+
+def solve_stream(mats, rhs, kinds, write_factors=False):
+    """Solve a ragged list of systems in one GPU call (the uneven stream).
+
+    mats: sequence of (n_i, n_i) float32 or float64 arrays (one dtype for all), n_i in 1..64;
+    rhs: sequence of (n_i,) or (n_i, k_i) arrays, k_i in 0..8 (None -> no right-hand side);
+    kinds: sequence of "cholesky"/"lu" (or 0/1). Returns (X list, info array), plus
+    (factors list, pivots list) when write_factors. Factors, pivots, info and X are
+    bit-identical to ``posv``/``gesv`` with backend="cuda" on each matrix.
+    """
+    import torch
+    from . import stream as _stream
+    if not has_cuda():
+        raise RuntimeError("solve_stream needs the CUDA backend")
+    count = len(mats)
+    if not (len(rhs) == count == len(kinds)):
+        raise ValueError("mats, rhs and kinds must have the same length")
+    if count == 0:
+        return ([], np.zeros(0, np.int32)) + (([], []) if write_factors else ())
+    dt = np.asarray(mats[0]).dtype
+    if dt not in (np.float32, np.float64):
+        raise TypeError("solve_stream takes float32 or float64 matrices")
+    kind = np.array([k if isinstance(k, (int, np.integer)) else {"cholesky": 0, "lu": 1}[k] for k in kinds], np.int8)
+    ns = np.array([np.asarray(a).shape[0] for a in mats], np.int32)
+    vec, bs = [], []
+    for a, b, n in zip(mats, rhs, ns):
+        a = np.asarray(a)
+        if a.shape != (n, n) or a.dtype != dt:
+            raise ValueError("every matrix must be square and of the first matrix's dtype")
+        if not 1 <= n <= 64:
+            raise ValueError("matrix size n outside supported range [1, 64]")
+        b = np.zeros((n, 0), dt) if b is None else np.asarray(b, dt)
+        vec.append(b.ndim == 1)
+        b = b.reshape(n, -1)
+        if b.shape[1] > 8:
+            raise ValueError("at most 8 right-hand sides per matrix")
+        bs.append(b)
+    nrhs = np.array([b.shape[1] for b in bs], np.int32)
+    aoff, boff, poff, *_ = _stream.layout(ns, nrhs)
+    dev = torch.device("cuda")
+    A = torch.from_numpy(np.concatenate([np.ascontiguousarray(a).ravel() for a in mats])).to(dev)
+    Bh = np.concatenate([b.ravel() for b in bs])
+    B = torch.from_numpy(Bh if Bh.size else np.zeros(1, dt)).to(dev)
+    piv = torch.zeros(int(ns.sum()), dtype=torch.int32, device=dev)
+    info = torch.zeros(count, dtype=torch.int32, device=dev)
+    t = lambda x, d: torch.from_numpy(np.ascontiguousarray(x, d)).to(dev)  # noqa: E731
+    _stream.solve(A, t(aoff.numpy(), np.int64), B, t(boff.numpy(), np.int64), piv, t(poff.numpy(), np.int64), info,
+                  t(ns, np.int32), t(nrhs, np.int32), t(kind, np.int8), write_factors=write_factors)
+    Xh, infoh = B.cpu().numpy(), info.cpu().numpy()
+    X = []
+    for i, (n, k) in enumerate(zip(ns, nrhs)):
+        x = Xh[boff[i]:boff[i] + n * k].reshape(n, k)
+        X.append(x[:, 0].copy() if vec[i] else x.copy())
+    if not write_factors:
+        return X, infoh
+    Ah, ph = A.cpu().numpy(), piv.cpu().numpy()
+    F = [Ah[aoff[i]:aoff[i] + n * n].reshape(n, n).copy() for i, n in enumerate(ns)]
+    P = [ph[poff[i]:poff[i] + n].copy() if kind[i] else None for i, n in enumerate(ns)]
+    return X, infoh, F, P

@@ -45,7 +45,10 @@ SIGNATURES.update({"tsdx_cuda_available": [], "tsdx_cuda_launch_count": [],
                    "tsdx_internal_div_check_f64": [_P, _P, _P, _P, _I64, _P],
                    "tsdx_internal_div_check_f32": [_P, _P, _P, _P, _I64, _P],
                    "tsdx_cuda_gesv_ir_f64": [_P, _I, _I64, _P, _P, _I, _I, C.c_double, _P, _P, _P, _P],
-                   "tsdx_cuda_posv_ir_f64": [_P, _I, _I64, _P, _P, _I, _I, C.c_double, _P, _P, _P, _P]})
+                   "tsdx_cuda_posv_ir_f64": [_P, _I, _I64, _P, _P, _I, _I, C.c_double, _P, _P, _P, _P],
+                   "tsdx_cuda_stream_scratch_bytes": [_I64],
+                   "tsdx_cuda_solve_stream_f32": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _I, C.c_uint, _P, _I64, _P],
+                   "tsdx_cuda_solve_stream_f64": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _I, C.c_uint, _P, _I64, _P]})
 
 _lib = None
 
@@ -60,7 +63,7 @@ def lib():
         for name, args in SIGNATURES.items():
             fn = getattr(L, name)
             fn.argtypes = args
-            fn.restype = C.c_int64 if name == "tsdx_cuda_launch_count" else C.c_int
+            fn.restype = C.c_int64 if name in ("tsdx_cuda_launch_count", "tsdx_cuda_stream_scratch_bytes") else C.c_int
         L.tsdx_cuda_last_error.restype = C.c_char_p
         _lib = L
     return _lib

@@ -18,12 +18,15 @@
 
 #include "../../include/tsdx_cuda.h"
 #include "launch.cuh"
+#include "stream.cuh"
 
 namespace tsdx {
 namespace host {
 
 int run_ir(bool spd, const double* A, int n, long long batch, double* B, const signed char* tier, int default_tier,
            int itmax, double tol, int* info, int* status, double* bwd, cudaStream_t st);
+long long stream_scratch_bytes(long long count);
+template <class T> int run_stream(dev::StreamArgs<T> a, void* scratch, long long scratch_bytes, cudaStream_t st);
 
 namespace {
 thread_local std::string g_err;
@@ -290,6 +293,52 @@ API int tsdx_cuda_posv_ir_f64(const double* A, int n, int64_t batch, double* B, 
                               int default_tier, int itmax, double tol, int* info, int* status, double* bwd,
                               void* stream) {
   return ir_entry(true, A, n, batch, B, tier, default_tier, itmax, tol, info, status, bwd, stream);
+}
+
+// ---- uneven stream -------------------------------------------------------------
+API int64_t tsdx_cuda_stream_scratch_bytes(int64_t count) {
+  return count < 0 ? 0 : tsdx::host::stream_scratch_bytes(count);
+}
+namespace {
+template <class T>
+int stream_entry(T* A, const int64_t* aoff, T* B, const int64_t* boff, int* piv, const int64_t* poff, int* info,
+                 const int* n, const int* nrhs, const signed char* kind, int64_t count, int write_factors,
+                 unsigned sched, void* scratch, int64_t scratch_bytes, void* st) {
+  if (count < 0 || count > (int64_t(1) << 31) - 1) return TSDX_ERR_BATCH;
+  if (count == 0) return TSDX_OK;
+  if (!A || !aoff || !n || !nrhs || !kind) return TSDX_ERR_NULL;
+  if (write_factors && (!piv || !poff)) return TSDX_ERR_NULL;
+  tsdx::dev::StreamArgs<T> a{};
+  a.A = A;
+  a.B = B;
+  a.piv = piv;
+  a.info = info;
+  a.aoff = reinterpret_cast<const long long*>(aoff);
+  a.boff = reinterpret_cast<const long long*>(boff);
+  a.poff = reinterpret_cast<const long long*>(poff);
+  a.n = n;
+  a.nrhs = nrhs;
+  a.kind = kind;
+  a.count = (int)count;
+  a.wf = write_factors ? 1 : 0;
+  a.sched = sched;
+  if (B && !boff) return TSDX_ERR_NULL;
+  return tsdx::host::run_stream<T>(a, scratch, scratch_bytes, ST(st));
+}
+}  // namespace
+API int tsdx_cuda_solve_stream_f32(float* A, const int64_t* aoff, float* B, const int64_t* boff, int* piv,
+                                   const int64_t* poff, int* info, const int* n, const int* nrhs,
+                                   const signed char* kind, int64_t count, int write_factors, unsigned sched,
+                                   void* scratch, int64_t scratch_bytes, void* stream) {
+  return stream_entry<float>(A, aoff, B, boff, piv, poff, info, n, nrhs, kind, count, write_factors, sched, scratch,
+                             scratch_bytes, stream);
+}
+API int tsdx_cuda_solve_stream_f64(double* A, const int64_t* aoff, double* B, const int64_t* boff, int* piv,
+                                   const int64_t* poff, int* info, const int* n, const int* nrhs,
+                                   const signed char* kind, int64_t count, int write_factors, unsigned sched,
+                                   void* scratch, int64_t scratch_bytes, void* stream) {
+  return stream_entry<double>(A, aoff, B, boff, piv, poff, info, n, nrhs, kind, count, write_factors, sched, scratch,
+                              scratch_bytes, stream);
 }
 
 #define TSDX_DEFINE(T, S)                                                                                      \

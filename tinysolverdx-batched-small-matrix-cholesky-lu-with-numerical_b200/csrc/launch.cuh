@@ -7,8 +7,7 @@
 #include <cstdint>
 #include <string>
 
-#include "chol_blk.cuh"
-#include "lu_blk.cuh"
+#include "blk.cuh"
 #include "solve.cuh"
 
 namespace tsdx {
@@ -62,20 +61,25 @@ int prepare(Kern kern, int smem) {
   return 0;
 }
 
-// Blocked one-warp-per-matrix LU / Cholesky (lu_blk.cuh, chol_blk.cuh): a
-// persistent CTA per SM with as many warps as shared memory holds (at most 16).
+// Blocked LU / Cholesky (blk.cuh): a persistent CTA per SM with as many warps as
+// shared memory holds (at most 16).
+template <class T, int NP, int NRHS>
+constexpr int blk_wpc() {
+  constexpr int FIT = (227 * 1024) / dev::BlkCfg<T, NP, NRHS>::WARPB;
+  return FIT < 1 ? 1 : (FIT > 16 ? 16 : FIT);
+}
+
 template <class T, int NP, int NRHS, bool CHOL>
-int launch_blk(const SolveArgs<T>& a, int vec, cudaStream_t st) {
+int launch_blk(const SolveArgs<T>& a, cudaStream_t st) {
   using C = dev::BlkCfg<T, NP, NRHS>;
-  constexpr int FIT = (227 * 1024) / C::WARPB;
-  constexpr int WPC = FIT < 1 ? 1 : (FIT > 16 ? 16 : FIT);
+  constexpr int WPC = blk_wpc<T, NP, NRHS>();
   constexpr int SMEM = WPC * C::WARPB;
-  auto kern = CHOL ? dev::chol_blk_kernel<T, NP, NRHS, WPC> : dev::lu_blk_kernel<T, NP, NRHS, WPC>;
+  auto kern = dev::blk_kernel<T, NP, NRHS, WPC, CHOL>;
   if (int rc = prepare(kern, SMEM)) return rc;
   const long long units = (a.batch + C::S - 1) / C::S;
   const long long ctas = (units + WPC - 1) / WPC;
   const int grid = grid_for(kern, SMEM, ctas, WPC * 32);
-  kern<<<grid, WPC * 32, SMEM, st>>>(a, FastDiv((unsigned)a.n), vec);
+  kern<<<grid, WPC * 32, SMEM, st>>>(a);
   launch_counter().fetch_add(1);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) { set_cuda_error(e, "kernel launch"); return -5; }
@@ -119,11 +123,8 @@ int launch_trs(const SolveArgs<T>& a, int vec, cudaStream_t st) {
 // One fused pass: factor A (and solve B columns [b0, b0 + nrhs), nrhs <= 8).
 template <class T, bool CHOL>
 int run_team(const SolveArgs<T>& a, cudaStream_t st) {
-  const int vec = vec_for<T>(a.A, a.n);
-  SolveArgs<T> b = a;
-  b.rowdiv = FastDiv((unsigned)(a.n * int(sizeof(T)) / vec));
   const int np = np_of(a.n), rb = nrhs_bucket(a.nrhs);
-  TSDX_NP_SWITCH(np, TSDX_RHS_SWITCH(rb, return (launch_blk<T, NP_, R_, CHOL>(b, vec, st))));
+  TSDX_NP_SWITCH(np, TSDX_RHS_SWITCH(rb, return (launch_blk<T, NP_, R_, CHOL>(a, st))));
   return 0;
 }
 
