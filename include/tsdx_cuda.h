@@ -40,6 +40,7 @@ extern "C" {
 #define TSDX_ERR_NRHS (-4)  /* nrhs < 0                                            */
 #define TSDX_ERR_CUDA (-5)  /* a CUDA runtime call failed; see tsdx_cuda_last_error */
 #define TSDX_ERR_NODEV (-6) /* no CUDA device is visible                           */
+#define TSDX_ERR_TOO_LARGE (-7) /* count above a fixed capacity; see tsdx_cuda_last_error */
 
 /* 1 if a CUDA device is visible (replaces tsdx::cuda::available, cuda_backend.hpp:9). */
 int tsdx_cuda_available(void);
@@ -141,6 +142,20 @@ int tsdx_cuda_solve_stream_f64(double* A, const int64_t* aoff, double* B, const 
                                const int64_t* poff, int* info, const int* n, const int* nrhs,
                                const signed char* kind, int64_t count, int write_factors, unsigned sched,
                                void* scratch, int64_t scratch_bytes, void* stream);
+
+/* ---- uneven stream without allocation (no reference counterpart) ------------------
+ * tsdx_cuda_solve_stream_f32 with the scratch in a fixed 1 MiB (+520 B) device array
+ * of the library instead of caller memory: allocates nothing. At most 262,144
+ * matrices per call; a larger count returns TSDX_ERR_TOO_LARGE before any launch.
+ * The array's address is looked up once per device on the first call on that device,
+ * which must not be made while the stream is being captured. The bucket counters
+ * that must start at zero are zeroed by every call on its stream. All calls on a
+ * device share the array: calls whose executions overlap (other streams or threads)
+ * race and corrupt each other's results, so order them (e.g. one stream). */
+int tsdx_cuda_solve_stream_noalloc_f32(float* A, const int64_t* aoff, float* B, const int64_t* boff, int* piv,
+                                       const int64_t* poff, int* info, const int* n, const int* nrhs,
+                                       const signed char* kind, int64_t count, int write_factors,
+                                       unsigned sched, void* stream);
 
 #ifdef __cplusplus
 }

@@ -38,3 +38,18 @@ def test_validation_without_device():
     # an empty batch is a successful no-op (batched.hpp:126)
     assert lib.tsdx_cuda_lu_batched_host_f64(capi.ptr(A), 4, 0, capi.ptr(piv), capi.ptr(info)) == capi.TSDX_OK
     assert lib.tsdx_cuda_getrf_f32(None, 4, 0, None, None, None) == capi.TSDX_ERR_NULL
+
+
+def test_stream_validation_without_device():
+    lib = capi.lib()
+    assert lib.tsdx_cuda_stream_scratch_bytes(10) == (4 * 32 + 2 + 10) * 4
+    assert lib.tsdx_cuda_stream_scratch_bytes(-1) == 0
+    nul = [None] * 10
+    assert lib.tsdx_cuda_solve_stream_f32(*nul, 0, 1, 0, None, 0, None) == capi.TSDX_OK
+    assert lib.tsdx_cuda_solve_stream_f64(*nul, -1, 1, 0, None, 0, None) == capi.TSDX_ERR_BATCH
+    assert lib.tsdx_cuda_solve_stream_f32(*nul, 5, 1, 0, None, 0, None) == capi.TSDX_ERR_NULL
+    # the no-allocation variant rejects a count above its fixed capacity first
+    assert lib.tsdx_cuda_solve_stream_noalloc_f32(*nul, (1 << 18) + 1, 1, 0, None) == capi.TSDX_ERR_TOO_LARGE
+    assert "262144" in capi.last_error()
+    assert lib.tsdx_cuda_solve_stream_noalloc_f32(*nul, -3, 1, 0, None) == capi.TSDX_ERR_BATCH
+    assert lib.tsdx_cuda_solve_stream_noalloc_f32(*nul, 0, 1, 0, None) == capi.TSDX_OK

@@ -19,6 +19,7 @@ TSDX_ERR_NULL = -3
 TSDX_ERR_NRHS = -4
 TSDX_ERR_CUDA = -5
 TSDX_ERR_NODEV = -6
+TSDX_ERR_TOO_LARGE = -7
 
 _P, _I, _I64 = C.c_void_p, C.c_int, C.c_int64
 
@@ -48,7 +49,8 @@ SIGNATURES.update({"tsdx_cuda_available": [], "tsdx_cuda_launch_count": [],
                    "tsdx_cuda_posv_ir_f64": [_P, _I, _I64, _P, _P, _I, _I, C.c_double, _P, _P, _P, _P],
                    "tsdx_cuda_stream_scratch_bytes": [_I64],
                    "tsdx_cuda_solve_stream_f32": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _I, C.c_uint, _P, _I64, _P],
-                   "tsdx_cuda_solve_stream_f64": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _I, C.c_uint, _P, _I64, _P]})
+                   "tsdx_cuda_solve_stream_f64": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _I, C.c_uint, _P, _I64, _P],
+                   "tsdx_cuda_solve_stream_noalloc_f32": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _I, C.c_uint, _P]})
 
 _lib = None
 
@@ -82,7 +84,9 @@ def check(rc, what=""):
         msg = {TSDX_ERR_N: "matrix size n outside supported range [1, 64]", TSDX_ERR_BATCH: "negative batch",
                TSDX_ERR_NULL: "null or misaligned pointer", TSDX_ERR_NRHS: "negative nrhs",
                TSDX_ERR_NODEV: "no CUDA device"}.get(rc)
-        if rc == TSDX_ERR_CUDA:
+        if rc in (TSDX_ERR_CUDA, TSDX_ERR_TOO_LARGE):
+            if rc == TSDX_ERR_TOO_LARGE:
+                raise ValueError(f"{what}: {last_error()}")
             raise RuntimeError(f"{what}: CUDA error: {last_error()}")
         if msg is None:
             raise RuntimeError(f"{what}: error {rc}")

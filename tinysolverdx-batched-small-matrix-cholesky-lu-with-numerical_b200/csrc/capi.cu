@@ -37,6 +37,7 @@ int g_sms[64] = {0};
 void set_cuda_error(cudaError_t e, const char* what) {
   g_err = std::string(what) + ": " + cudaGetErrorString(e);
 }
+void set_error_message(const std::string& msg) { g_err = msg; }
 std::atomic<long long>& launch_counter() { return g_launches; }
 
 int device_sms(int dev) {

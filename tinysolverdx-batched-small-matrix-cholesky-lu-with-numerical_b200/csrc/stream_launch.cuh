@@ -25,7 +25,7 @@ template <class T> constexpr int stream_warpb() {
 }
 }  // namespace
 
-inline long long stream_scratch_bytes_of(long long count) { return (4LL * dev::kStreamBuckets + 2 + count) * 4; }
+constexpr long long stream_scratch_bytes_of(long long count) { return (4LL * dev::kStreamBuckets + 2 + count) * 4; }
 
 template <class T>
 int run_stream(dev::StreamArgs<T> a, void* scratch, long long scratch_bytes, cudaStream_t st) {
