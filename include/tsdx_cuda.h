@@ -145,7 +145,10 @@ int tsdx_cuda_solve_stream_f64(double* A, const int64_t* aoff, double* B, const 
 
 /* ---- uneven stream without allocation (no reference counterpart) ------------------
  * tsdx_cuda_solve_stream_f32 with the scratch in a fixed 1 MiB (+520 B) device array
- * of the library instead of caller memory: allocates nothing. At most 262,144
+ * of the library instead of caller memory: allocates nothing, for callers that may
+ * not allocate device memory at call time (memory owned by another allocator or
+ * reserved up front; request paths where cudaMalloc could stall or fail). Every GPU
+ * that loads the library keeps the array until exit. At most 262,144
  * matrices per call; a larger count returns TSDX_ERR_TOO_LARGE before any launch.
  * The array's address is looked up once per device on the first call on that device,
  * which must not be made while the stream is being captured. The bucket counters

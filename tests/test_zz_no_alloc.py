@@ -3,6 +3,11 @@ allocation) against tsdx_cuda_solve_stream_f32 with caller scratch: two calls in
 row on different streams of matrices, bit-identical factors, pivots, info and X;
 a count above the fixed capacity is rejected before anything runs.
 
+The entry point exists for callers that may not allocate device memory when they
+call (their memory belongs to another allocator, or an allocation could stall or
+fail mid-request); the second call checks that nothing left in the shared array by
+the first call leaks into its results.
+
 Kept in its own file, named to be collected last, so that it also runs after every
 other test has used the library on the same device."""
 import numpy as np

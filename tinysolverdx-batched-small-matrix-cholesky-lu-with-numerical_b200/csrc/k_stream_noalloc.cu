@@ -2,6 +2,17 @@
 // scratch in a fixed device array of this module instead of caller memory or an
 // allocation on the stream. It has no TinySolverDx counterpart.
 //
+// Who needs it: callers that may not allocate device memory at call time. A host
+// application whose memory is owned by another allocator (a framework's caching
+// pool, a serving process that reserves all device memory up front) cannot hand
+// out cudaMalloc'd scratch without going around that owner, and a latency-bound
+// caller cannot afford cudaMalloc/cudaFree, which may synchronise the device or
+// fail under memory pressure in the middle of a request. Those callers pass only
+// their inputs and outputs here.
+//
+// Cost: every GPU that loads the library holds the array (about 1 MiB) until the
+// process exits, whether or not this entry point is ever called.
+//
 // Scratch: kNoAllocMaxCount matrices at most (262,144; 1 MiB of sort permutation
 // plus 520 bytes of bucket counters). Its device address is looked up once per
 // device with cudaGetSymbolAddress on the first call on that device (that first
