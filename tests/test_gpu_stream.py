@@ -97,7 +97,7 @@ def run_direct(n, nrhs, kind, A, B, wf=True, sched=0, scratch=True):
 
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
-@pytest.mark.parametrize("sched", [0, 3])
+@pytest.mark.parametrize("sched", [0, 15, 5])
 def test_stream_bit_identical_to_dense(dtype, sched):
     n, nrhs, kind, mats, bs, A, B = make_stream(11 + sched, 1500, dtype)
     ref = dense_reference(n, nrhs, kind, mats, bs, dtype)
@@ -159,7 +159,7 @@ def test_plan_autotune_graph_replay():
     plan = stream.StreamPlan(n, nrhs, kind, torch.float32)
     B = B[:-1]  # drop make_stream's trailing pad element
     best = plan.tune(A, B, reps=2)
-    assert best in stream.SCHEDULES and set(plan.timings) == set(stream.SCHEDULES)
+    assert 0 <= best < (1 << stream.SCHED_BITS) and len(plan.timings) >= 2
     plan.capture()
     for _ in range(2):  # replay twice on fresh inputs
         plan.load(A, B)

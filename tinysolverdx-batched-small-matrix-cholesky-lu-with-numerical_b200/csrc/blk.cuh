@@ -51,7 +51,7 @@ struct BlkCfg {
   static constexpr int SEGB = (MAT + AUX + 127) / 128 * 128;
   static constexpr int WARPB = S * SEGB;
   static_assert(NP % PB == 0, "panel width divides the padded order");
-  static_assert(MR <= 2, "at most two row slots per lane");
+  static_assert(MR <= 4, "at most four row slots per lane");
 };
 
 // One matrix for one segment. Every pointer may be null when the job is not live.
@@ -164,7 +164,9 @@ __device__ __forceinline__ void seg_backsolve(unsigned char* M, const int* ord, 
 #pragma unroll
     for (int c = 0; c < NRHS; ++c) {
       T y = yv[0][c] * dv[0];
-      if (MR > 1 && ks == MR - 1) y = yv[MR - 1][c] * dv[MR - 1];
+#pragma unroll
+      for (int t = 1; t < MR; ++t)
+        if (ks == t) y = yv[t][c] * dv[t];
       x[c] = __shfl_sync(kFull, y, kl);
     }
 #pragma unroll
@@ -262,7 +264,8 @@ __device__ __forceinline__ void lu_matrix(unsigned char* M, const MatJob<T>& j, 
 #pragma unroll
       for (int jj = i; jj < PB; ++jj) {
         T v = pan[0][jj];
-        if (MR > 1) v = (wslot == MR - 1) ? pan[MR - 1][jj] : v;
+#pragma unroll
+        for (int t = 1; t < MR; ++t) v = (wslot == t) ? pan[t][jj] : v;
         uw[jj] = __shfl_sync(kFull, v, wl);
       }
       if (lane == wl) {
@@ -417,7 +420,8 @@ __device__ __forceinline__ void chol_matrix(unsigned char* M, const MatJob<T>& j
       const int k = k0 + i;
       const int dl = segbase + (k & (G - 1)), ds = k / G;
       T dv = pan[0][i];
-      if (MR > 1) dv = (ds == MR - 1) ? pan[MR - 1][i] : dv;
+#pragma unroll
+      for (int t = 1; t < MR; ++t) dv = (ds == t) ? pan[t][i] : dv;
       const T d = __shfl_sync(kFull, dv, dl);
       const bool bad = !(d > T(0));
       info = (bad && info == 0) ? k + 1 : info;
@@ -433,7 +437,8 @@ __device__ __forceinline__ void chol_matrix(unsigned char* M, const MatJob<T>& j
       for (int jj = i + 1; jj < PB; ++jj) {
         const int rj = k0 + jj;
         T v = pan[0][i];
-        if (MR > 1) v = ((rj / G) == MR - 1) ? pan[MR - 1][i] : v;
+#pragma unroll
+        for (int t = 1; t < MR; ++t) v = ((rj / G) == t) ? pan[t][i] : v;
         const T lj = __shfl_sync(kFull, v, segbase + (rj & (G - 1)));
 #pragma unroll
         for (int s = 0; s < MR; ++s) {
@@ -565,9 +570,9 @@ __device__ __forceinline__ void blk_matrix(unsigned char* M, const MatJob<T>& j,
 // Dense batch: one persistent CTA of WPC warps per SM slot; every round each
 // segment takes the next matrix and the CTA walks the code together, so the
 // instruction stream fetched for one warp serves all of them.
-template <class T, int NP, int NRHS, int WPC, bool CHOL>
+template <class T, int NP, int NRHS, int WPC, bool CHOL, int GO = 0>
 __global__ void __launch_bounds__(WPC * 32, 1) blk_kernel(SolveArgs<T> p) {
-  using C = BlkCfg<T, NP, NRHS>;
+  using C = BlkCfg<T, NP, NRHS, GO>;
   constexpr int G = C::G, S = C::S;
   extern __shared__ __align__(128) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -595,7 +600,7 @@ __global__ void __launch_bounds__(WPC * 32, 1) blk_kernel(SolveArgs<T> p) {
     j.ldb = p.ldb;
     j.b0 = p.b0;
     j.nrhs = p.nrhs;
-    blk_matrix<T, NP, NRHS, CHOL>(M, j, g);
+    blk_matrix<T, NP, NRHS, CHOL, GO>(M, j, g);
   }
 }
 

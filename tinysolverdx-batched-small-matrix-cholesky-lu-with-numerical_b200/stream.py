@@ -19,9 +19,9 @@ import torch
 from . import capi
 
 CHOLESKY, LU = 0, 1
-# sched bits: 1 -> n <= 8 matrices one per warp (else four per warp);
-#             2 -> 9 <= n <= 16 one per warp (else two per warp)
-SCHEDULES = (0, 1, 2, 3)
+# sched bit c (order class c: n in 1..8, 9..16, 17..24, 25..32) set -> those matrices
+# run one per warp; clear -> four (class 0) or two (classes 1-3) share a warp
+SCHED_BITS = 4
 
 
 def layout(n, nrhs, device=None):
@@ -124,22 +124,32 @@ class StreamPlan:
         solve(self.A, self.aoff, self.B, self.boff, self.piv, self.poff, self.info, self.n, self.nrhs, self.kind,
               self.write_factors, self.sched if sched is None else sched, self.scratch, stream)
 
-    def tune(self, A, B, reps=3, schedules=SCHEDULES):
-        """Time each schedule on (A, B) with CUDA events and keep the fastest."""
-        A0, B0 = A.reshape(-1).to(self.device), B.reshape(-1).to(self.device)
+    def _time(self, A0, B0, sched, reps):
         s = torch.cuda.current_stream(self.device)
-        for sc in schedules:
-            best = float("inf")
-            for _ in range(reps):
-                self.load(A0, B0)
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(s)
-                self.launch(sc, s)
-                e1.record(s)
-                e1.synchronize()
-                best = min(best, e0.elapsed_time(e1))
-            self.timings[sc] = best
-        self.sched = min(self.timings, key=self.timings.get)
+        best = float("inf")
+        for _ in range(reps):
+            self.load(A0, B0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            self.launch(sched, s)
+            e1.record(s)
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        self.timings[sched] = best
+        return best
+
+    def tune(self, A, B, reps=3):
+        """Pick the warp schedule: starting from all-packed, flip each order class to
+        one matrix per warp in turn and keep the flip when it times faster on (A, B)."""
+        A0, B0 = A.reshape(-1).to(self.device), B.reshape(-1).to(self.device)
+        self.timings = {}
+        sched = 0
+        best = self._time(A0, B0, sched, reps)
+        for c in range(SCHED_BITS):
+            t = self._time(A0, B0, sched | (1 << c), reps)
+            if t < best:
+                sched, best = sched | (1 << c), t
+        self.sched = sched
         self.graph = None
         return self.sched
 
