@@ -119,6 +119,29 @@ int tsdx_cuda_posv_ir_f64(const double* A, int n, int64_t batch, double* B, cons
                           int default_tier, int itmax, double tol, int* info, int* status, double* bwd,
                           void* stream);
 
+/* ---- learned precision-tier selector (no reference counterpart) -------------------
+ * A 24 -> 64 -> 64 -> 4 MLP over cheap per-matrix features predicts the cheapest
+ * tier (0 fp16, 1 bf16, 2 fp32, 3 fp64) whose refinement converges; the tier array
+ * feeds tsdx_cuda_gesv_ir_f64 / tsdx_cuda_posv_ir_f64. All pointers are device
+ * pointers, float32 unless stated; the parameter vector (6020 floats) is laid out
+ * W1[24][64], b1[64], W2[64][64], b2[64], W3[64][4], b3[4]; norm = mu[24], 1/sd[24].
+ *   features: 24 per matrix of the float64 stack A (batch, n, n); kind (batch) int8
+ *             0 SPD / 1 general, or NULL to use kind_all for every matrix.
+ *   forward:  logits (batch, 4) and/or argmax tier (batch) int8; either may be NULL.
+ *   grad:     gradient of sum_s w[y_s] CE_s / batch (class_weight (4) or NULL for 1)
+ *             and the loss; scratch >= tsdx_cuda_mlp_scratch_bytes(batch) bytes.
+ *   adam:     one Adam step (bias-corrected, step >= 1) on count parameters. */
+int tsdx_cuda_selector_features_f64(const double* A, int n, int64_t batch, const signed char* kind, int kind_all,
+                                    float* features, void* stream);
+int tsdx_cuda_mlp_forward(const float* params, const float* norm, const float* features, int64_t batch,
+                          float* logits, signed char* tier, void* stream);
+int64_t tsdx_cuda_mlp_scratch_bytes(int64_t batch);
+int tsdx_cuda_mlp_grad(const float* params, const float* norm, const float* features, const signed char* label,
+                       const float* class_weight, int64_t batch, float* grad, float* loss, void* scratch,
+                       int64_t scratch_bytes, void* stream);
+int tsdx_cuda_adam_step(float* params, const float* grad, float* m, float* v, int64_t count, float lr,
+                        float beta1, float beta2, float eps, int step, void* stream);
+
 /* ---- uneven stream (no reference counterpart) -------------------------------------
  * One call over `count` matrices of mixed order n in [1, 64], Cholesky (kind 0, posv)
  * and LU (kind 1, gesv) mixed, 0..8 right-hand sides each, all in device memory:

@@ -13,6 +13,7 @@ import argparse
 import concurrent.futures as cf
 import os
 import pathlib
+import re
 import subprocess
 import sys
 import sysconfig
@@ -27,18 +28,25 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden",
                   "-I" + str(CSRC), "-I" + str(ROOT / "include")]
-CUDA_SOURCES = ["capi.cu", "k_lu_f32.cu", "k_lu_f64.cu", "k_chol_f32.cu", "k_chol_f64.cu", "k_ir.cu", "k_stream_f32.cu", "k_stream_f64.cu", "k_stream_noalloc.cu"]
+CUDA_SOURCES = ["capi.cu", "k_lu_f32.cu", "k_lu_f64.cu", "k_chol_f32.cu", "k_chol_f64.cu", "k_ir.cu", "k_stream_f32.cu", "k_stream_f64.cu", "k_stream_noalloc.cu", "k_selector.cu"]
 
 
-def _newest_header():
-    hs = list(CSRC.glob("*.cuh")) + list((ROOT / "include").glob("*.h"))
-    return max((h.stat().st_mtime for h in hs), default=0.0)
+def _deps(path, seen=None):
+    """The file and every local header it includes, transitively (#include "...")."""
+    seen = set() if seen is None else seen
+    path = path.resolve()
+    if path in seen or not path.exists():
+        return seen
+    seen.add(path)
+    for m in re.finditer(r'^\s*#\s*include\s+"([^"]+)"', path.read_text(), re.M):
+        _deps(path.parent / m.group(1), seen)
+    return seen
 
 
 def _compile(src, force):
     obj = OBJ / (pathlib.Path(src).stem + ".o")
     s = CSRC / src
-    if not force and obj.exists() and obj.stat().st_mtime >= max(s.stat().st_mtime, _newest_header()):
+    if not force and obj.exists() and obj.stat().st_mtime >= max(d.stat().st_mtime for d in _deps(s)):
         return obj, None
     cmd = [NVCC] + NVFLAGS + ["-c", str(s), "-o", str(obj)]
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -50,7 +50,13 @@ SIGNATURES.update({"tsdx_cuda_available": [], "tsdx_cuda_launch_count": [],
                    "tsdx_cuda_stream_scratch_bytes": [_I64],
                    "tsdx_cuda_solve_stream_f32": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _I, C.c_uint, _P, _I64, _P],
                    "tsdx_cuda_solve_stream_f64": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _I, C.c_uint, _P, _I64, _P],
-                   "tsdx_cuda_solve_stream_noalloc_f32": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _I, C.c_uint, _P]})
+                   "tsdx_cuda_solve_stream_noalloc_f32": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _I, C.c_uint, _P],
+                   "tsdx_cuda_selector_features_f64": [_P, _I, _I64, _P, _I, _P, _P],
+                   "tsdx_cuda_mlp_forward": [_P, _P, _P, _I64, _P, _P, _P],
+                   "tsdx_cuda_mlp_scratch_bytes": [_I64],
+                   "tsdx_cuda_mlp_grad": [_P, _P, _P, _P, _P, _I64, _P, _P, _P, _I64, _P],
+                   "tsdx_cuda_adam_step": [_P, _P, _P, _P, _I64, C.c_float, C.c_float, C.c_float, C.c_float, _I,
+                                           _P]})
 
 _lib = None
 
@@ -65,7 +71,8 @@ def lib():
         for name, args in SIGNATURES.items():
             fn = getattr(L, name)
             fn.argtypes = args
-            fn.restype = C.c_int64 if name in ("tsdx_cuda_launch_count", "tsdx_cuda_stream_scratch_bytes") else C.c_int
+            fn.restype = C.c_int64 if name in ("tsdx_cuda_launch_count", "tsdx_cuda_stream_scratch_bytes",
+                                               "tsdx_cuda_mlp_scratch_bytes") else C.c_int
         L.tsdx_cuda_last_error.restype = C.c_char_p
         _lib = L
     return _lib

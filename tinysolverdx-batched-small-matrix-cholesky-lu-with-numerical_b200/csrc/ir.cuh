@@ -5,14 +5,19 @@
 //   1. A (fp64, global) is read once, coalesced, and written to shared memory as
 //      an fp32 working matrix, scaled by powers of two (rows then columns, max
 //      |a| -> 1, exact) so fp16 tensor-core operands stay in range.
-//   2. The scaled matrix is factored in fp32 with partial pivoting (LU) or
-//      without (Cholesky): 16-column panels in registers, the trailing update
+//   2. The scaled matrix is factored in fp32 with partial pivoting (LU) or, for
+//      symmetric positive definite input, without pivoting (A = L U with U = D L^T,
+//      the Cholesky factor up to a diagonal: SPD matrices need no pivoting, and the
+//      shared code keeps one fast path): 16-column panels in registers, the trailing update
 //      A22 -= L21 U12 either on the tensor cores (mma.sync m16n8k16, fp16 or bf16
 //      operands, fp32 accumulation) or on the fp32 CUDA cores, by tier.
-//   3. x0 = A^{-1} b with the low-precision factors (fp32 triangular solves).
-//   4. Refinement: r = b - A x in fp64 straight from A in global memory, normwise
-//      backward error ||r|| / (||A||_F ||x|| + ||b||) (runtime.cpp:230-242); stop
-//      when it is <= tol, else x += A^{-1} r with the same factors.
+//   3. x0 = A^{-1} b with the low-precision factors (fp32 triangular solves,
+//      reciprocal pivots computed once after the factorization).
+//   4. Refinement: r = b - A x in fp64 straight from A in global memory (rows
+//      read coalesced, 32 row sums per lane folded by a transposing butterfly),
+//      normwise backward error ||r|| / (||A||_F ||x|| + ||b||)
+//      (runtime.cpp:230-242); stop when it is <= tol, else x += A^{-1} r with the
+//      same factors.
 // A matrix that does not converge within itmax steps (or meets a zero / non-
 // positive pivot in low precision) is reported with status -1; the host then
 // solves it with the plain fp64 kernel (the fallback is never silent).
@@ -67,25 +72,33 @@ struct IrCfg {
   static constexpr int PB = 16;
   static constexpr int RSF = NP * 4 + 16;  // fp32 row: an odd number of 16-byte units
   static constexpr int F = NP * RSF;
-  static constexpr int AUX = NP * 4 /*ord*/ + NP * 8 /*x*/ + NP * 4 /*col scale*/ + 32;
+  // ord (int), x (double), column scales, row scales, reciprocal pivots (float)
+  static constexpr int AUX = NP * 4 + NP * 8 + NP * 4 * 3 + 32;
   static constexpr int WARPB = (F + AUX + 127) / 128 * 128;
+  // cooperative float4 passes: CG groups of 4 columns, RPI rows per pass
+  static constexpr int CG = NP / 4;
+  static constexpr int CGP = CG <= 4 ? 4 : CG <= 8 ? 8 : 16;
+  static constexpr int RPI = 32 / CGP;
   static_assert(NP % 16 == 0, "tensor-core tiles need NP % 16 == 0");
 };
 
 template <int NP, bool SPD, int WPC>
 __global__ void __launch_bounds__(WPC * 32, 1) ir_kernel(IrArgs p) {
   using C = IrCfg<NP>;
-  constexpr int MR = C::MR, PB = C::PB, RSF = C::RSF;
+  constexpr int MR = C::MR, PB = C::PB, RSF = C::RSF, CG = C::CG, CGP = C::CGP, RPI = C::RPI;
   extern __shared__ __align__(128) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned char* Fb = smem + warp * C::WARPB;
   int* ord = reinterpret_cast<int*>(Fb + C::F);
   double* xs = reinterpret_cast<double*>(Fb + C::F + NP * 4);
   float* csc = reinterpret_cast<float*>(Fb + C::F + NP * 12);
+  float* rsd = csc + NP;
+  float* rinv = rsd + NP;
   auto F = [&](int r, int c) -> float& { return *reinterpret_cast<float*>(Fb + r * RSF + c * 4); };
   auto F4 = [&](int r, int c) -> float4& { return *reinterpret_cast<float4*>(Fb + r * RSF + c * 4); };
   const int n = p.n;
   const long long per_round = (long long)gridDim.x * WPC;
+  const int q4 = lane % CGP, rho = lane / CGP;  // cooperative pass coordinates
 
   for (long long base = (long long)blockIdx.x * WPC; base < p.batch; base += per_round) {
     __syncthreads();
@@ -106,66 +119,86 @@ __global__ void __launch_bounds__(WPC * 32, 1) ir_kernel(IrArgs p) {
     double afro = 0.0;
     float rsc[MR];
     {
-      // row scales: lane r holds rows r, r+32; one coalesced row read per step
-      float rmax[MR];
-#pragma unroll
-      for (int s = 0; s < MR; ++s) rmax[s] = 0.f;
+      // coalesced row reads (lane c holds columns c, c + 32), unscaled fp32 copy
+#pragma unroll 4
       for (int r = 0; r < n; ++r) {
         const double* row = Ag + (long long)r * n;
-        float mx = 0.f;
-        for (int c = lane; c < n; c += 32) {
-          const double v = row[c];
-          afro = fma(v, v, afro);
-          mx = fmaxf(mx, (float)fabs(v));
-          F(r, c) = (float)v;
+#pragma unroll
+        for (int s = 0; s < MR; ++s) {
+          const int c = lane + 32 * s;
+          if (c < n) {
+            const double v = __ldg(row + c);
+            afro = fma(v, v, afro);
+            F(r, c) = (float)v;
+          }
         }
-        for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, o));
-#pragma unroll
-        for (int s = 0; s < MR; ++s)
-          if (r == lane + 32 * s) rmax[s] = mx;
       }
+      if (n < NP) {  // identity padding
+        for (int r = 0; r < NP; ++r)
 #pragma unroll
-      for (int s = 0; s < MR; ++s) {
-        int e = 0;
-        frexpf(rmax[s], &e);
-        rsc[s] = (rmax[s] > 0.f && isfinite(rmax[s])) ? ldexpf(1.f, -e) : 1.f;
+          for (int s = 0; s < MR; ++s) {
+            const int c = lane + 32 * s;
+            if (c < NP && (r >= n || c >= n)) F(r, c) = (r == c) ? 1.f : 0.f;
+          }
       }
       for (int o = 16; o > 0; o >>= 1) afro += __shfl_xor_sync(kFull, afro, o);
       __syncwarp();
-      // apply row scales (each lane its rows), identity-pad rows/cols >= n
+      // row scales: each lane scans its own rows with 16-byte reads
 #pragma unroll
       for (int s = 0; s < MR; ++s) {
         const int r = lane + 32 * s;
-        if (r >= NP) continue;
-        for (int c = 0; c < NP; ++c) {
-          if (r < n && c < n) F(r, c) *= rsc[s];
-          else F(r, c) = (r == c) ? 1.f : 0.f;
-        }
-      }
-      __syncwarp();
-      // column scales (SPD keeps symmetry: scale columns by the row scale)
-      for (int c = lane; c < NP; c += 32) {
         float mx = 0.f;
-        for (int r = 0; r < n; ++r) mx = fmaxf(mx, fabsf(F(r, c)));
+        if (r < n) {
+#pragma unroll
+          for (int c = 0; c < NP; c += 4) {
+            const float4 v = F4(r, c);
+            mx = fmaxf(mx, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
+          }
+        }
         int e = 0;
         frexpf(mx, &e);
-        float cs = (c < n && mx > 0.f && isfinite(mx)) ? ldexpf(1.f, -e) : 1.f;
-        csc[c] = cs;
+        rsc[s] = (r < n && mx > 0.f && isfinite(mx)) ? ldexpf(1.f, -e) : 1.f;
+        if (r < NP) rsd[r] = rsc[s];
       }
       __syncwarp();
-      if (SPD) {
-        for (int c = lane; c < NP; c += 32) {
-          // D A D with D = row scales keeps the matrix symmetric
-          float d = 1.f;
-#pragma unroll
-          for (int s = 0; s < MR; ++s)
-            if (c == lane + 32 * s) d = rsc[s];
-          csc[c] = d;
+      // apply the row scales and take column maxima (lanes: 4 columns x RPI rows)
+      float cm[4] = {0.f, 0.f, 0.f, 0.f};
+      if (q4 < CG) {
+        for (int r = rho; r < NP; r += RPI) {
+          float4 v = F4(r, 4 * q4);
+          const float sc = rsd[r];
+          v.x *= sc; v.y *= sc; v.z *= sc; v.w *= sc;
+          F4(r, 4 * q4) = v;
+          cm[0] = fmaxf(cm[0], fabsf(v.x));
+          cm[1] = fmaxf(cm[1], fabsf(v.y));
+          cm[2] = fmaxf(cm[2], fabsf(v.z));
+          cm[3] = fmaxf(cm[3], fabsf(v.w));
         }
-        __syncwarp();
       }
-      for (int r = 0; r < n; ++r)
-        for (int c = lane; c < n; c += 32) F(r, c) *= csc[c];
+#pragma unroll
+      for (int o = CGP; o < 32; o <<= 1)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) cm[i] = fmaxf(cm[i], __shfl_xor_sync(kFull, cm[i], o));
+      if (rho == 0 && q4 < CG) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int c = 4 * q4 + i;
+          int e = 0;
+          frexpf(cm[i], &e);
+          // SPD keeps symmetry: D A D with D the row scales
+          const float cs = SPD ? rsd[c] : ((c < n && cm[i] > 0.f && isfinite(cm[i])) ? ldexpf(1.f, -e) : 1.f);
+          csc[c] = cs;
+        }
+      }
+      __syncwarp();
+      if (q4 < CG) {
+        const float4 cs = *reinterpret_cast<const float4*>(csc + 4 * q4);
+        for (int r = rho; r < NP; r += RPI) {
+          float4 v = F4(r, 4 * q4);
+          v.x *= cs.x; v.y *= cs.y; v.z *= cs.z; v.w *= cs.w;
+          F4(r, 4 * q4) = v;
+        }
+      }
       __syncwarp();
     }
     double bv[MR];
@@ -204,32 +237,9 @@ __global__ void __launch_bounds__(WPC * 32, 1) ir_kernel(IrArgs p) {
 #pragma unroll
       for (int i = 0; i < PB; ++i) {
         const int k = k0 + i;
-        if (SPD) {
-          const int ds = k >> 5, dl = k & 31;
-          float dv = pan[0][i];
-          if (MR > 1 && ds == 1) dv = pan[MR - 1][i];
-          const float d = __shfl_sync(kFull, dv, dl);
-          if (!(d > 0.f) && info == 0) info = k + 1;
-          const float lkk = sqrtf(d > 0.f ? d : 1.f);
-          const float ry = 1.f / lkk;
-#pragma unroll
-          for (int s = 0; s < MR; ++s) {
-            const int r = lane + 32 * s;
-            if (r == k) pan[s][i] = lkk;
-            else if (r > k) pan[s][i] *= ry;
-          }
-#pragma unroll
-          for (int j = i + 1; j < PB; ++j) {
-            const int rj = k0 + j;
-            float v = pan[0][i];
-            if (MR > 1 && (rj >> 5) == 1) v = pan[MR - 1][i];
-            const float lj = __shfl_sync(kFull, v, rj & 31);
-#pragma unroll
-            for (int s = 0; s < MR; ++s)
-              if (lane + 32 * s >= rj) pan[s][j] = fmaf(-pan[s][i], lj, pan[s][j]);
-          }
-          if (lane == 0) ord[k] = k;
-        } else {
+        {
+          int bpos = k;  // SPD: no pivoting (A = L U with U = D L^T)
+          if (!SPD) {
           unsigned bk = 0;
           int bp = 0x7fffffff;
 #pragma unroll
@@ -240,7 +250,8 @@ __global__ void __launch_bounds__(WPC * 32, 1) ir_kernel(IrArgs p) {
             bp = (act[s] && better) ? pos[s] : bp;
           }
           const unsigned mk = __reduce_max_sync(kFull, bk);
-          const int bpos = __reduce_min_sync(kFull, bk == mk ? bp : 0x7fffffff);
+          bpos = __reduce_min_sync(kFull, bk == mk ? bp : 0x7fffffff);
+          }
           int myslot = -1;
 #pragma unroll
           for (int s = 0; s < MR; ++s) myslot = (act[s] && pos[s] == bpos) ? s : myslot;
@@ -250,7 +261,8 @@ __global__ void __launch_bounds__(WPC * 32, 1) ir_kernel(IrArgs p) {
 #pragma unroll
           for (int j = i; j < PB; ++j) {
             float v = pan[0][j];
-            if (MR > 1 && wslot == 1) v = pan[MR - 1][j];
+#pragma unroll
+            for (int t2 = 1; t2 < MR; ++t2) v = (wslot == t2) ? pan[t2][j] : v;
             uw[j] = __shfl_sync(kFull, v, wl);
           }
           if (lane == wl) ord[k] = lane + 32 * wslot;
@@ -261,7 +273,7 @@ __global__ void __launch_bounds__(WPC * 32, 1) ir_kernel(IrArgs p) {
             pos[s] = win ? k : (atk ? bpos : pos[s]);
             act[s] = act[s] && !win;
           }
-          const bool zero = !(uw[i] != 0.f) || !isfinite(uw[i]);
+          const bool zero = SPD ? (!(uw[i] > 0.f) || !isfinite(uw[i])) : (!(uw[i] != 0.f) || !isfinite(uw[i]));
           if (zero && info == 0) info = k + 1;
           const float ry = zero ? 0.f : 1.f / uw[i];
 #pragma unroll
@@ -285,37 +297,41 @@ __global__ void __launch_bounds__(WPC * 32, 1) ir_kernel(IrArgs p) {
       __syncwarp();
       const int j1 = k0 + PB;
       if (j1 >= NP) continue;
-      if (!SPD) {
+      int ordp[PB];  // physical rows of the panel's pivots
+#pragma unroll
+      for (int i = 0; i < PB; ++i) ordp[i] = ord[k0 + i];
+      {
         // U12: the panel's pivot rows on the trailing columns (unit-lower solve)
         for (int j = j1 + lane; j < NP; j += 32) {
           float u[PB];
 #pragma unroll
           for (int i = 0; i < PB; ++i) {
-            const int pr = ord[k0 + i];
-            float acc = F(pr, j);
+            float acc = F(ordp[i], j);
 #pragma unroll
-            for (int i2 = 0; i2 < i; ++i2) acc = fmaf(-F(pr, k0 + i2), u[i2], acc);
+            for (int i2 = 0; i2 < i; ++i2) acc = fmaf(-F(ordp[i], k0 + i2), u[i2], acc);
             u[i] = acc;
-            if (i > 0) F(pr, j) = acc;
+            if (i > 0) F(ordp[i], j) = acc;
           }
         }
         __syncwarp();
       }
-      // trailing update of the rows still active (SPD: lower triangle rows >= j1)
+      // trailing update of the rows still active
       if (tc) {
         const int g = lane >> 2, tq = lane & 3;
 #pragma unroll
         for (int rt = 0; rt < NP / 16; ++rt) {
           const int ra = rt * 16 + g, rb = ra + 8;
-          // skip row tiles with no row to update
-          bool upd_a = false, upd_b = false;
-          if (SPD) {
-            upd_a = ra >= j1;
-            upd_b = rb >= j1;
-          } else {
-            // active after the panel: not yet retired (final position >= j1)
-            upd_a = true;
-            upd_b = true;
+          // rows still being updated: those not yet retired
+          bool sa, sb;
+          {
+            int va = act[0], vb = act[0];
+#pragma unroll
+            for (int t2 = 1; t2 < MR; ++t2) {
+              va = ((ra >> 5) == t2) ? (int)act[t2] : va;
+              vb = ((rb >> 5) == t2) ? (int)act[t2] : vb;
+            }
+            sa = __shfl_sync(kFull, va, ra & 31) != 0;
+            sb = __shfl_sync(kFull, vb, rb & 31) != 0;
           }
           // L21 fragment (negated): rows ra/rb, panel columns k0 + [2tq, 2tq+1, 2tq+8, 2tq+9]
           unsigned af[4];
@@ -325,119 +341,156 @@ __global__ void __launch_bounds__(WPC * 32, 1) ir_kernel(IrArgs p) {
           af[3] = pack2(-F(rb, k0 + 2 * tq + 8), -F(rb, k0 + 2 * tq + 9), f16);
           for (int ct = j1 / 8; ct < NP / 8; ++ct) {
             const int c0 = ct * 8 + 2 * tq;
-            if (SPD && ct * 8 > rt * 16 + 15) break;  // tile entirely above the diagonal
-            // U12 fragment: B[k][n] = U(k0+k, col ct*8+g); SPD: L(col, k0+k)
+            // U12 fragment: B[k][n] = U(k0+k, col ct*8+g)
             unsigned bf[2];
             const int cg = ct * 8 + g;
-            if (SPD) {
-              bf[0] = pack2(F(cg, k0 + 2 * tq), F(cg, k0 + 2 * tq + 1), f16);
-              bf[1] = pack2(F(cg, k0 + 2 * tq + 8), F(cg, k0 + 2 * tq + 9), f16);
-            } else {
-              bf[0] = pack2(F(ord[k0 + 2 * tq], cg), F(ord[k0 + 2 * tq + 1], cg), f16);
-              bf[1] = pack2(F(ord[k0 + 2 * tq + 8], cg), F(ord[k0 + 2 * tq + 9], cg), f16);
-            }
+            bf[0] = pack2(F(ord[k0 + 2 * tq], cg), F(ord[k0 + 2 * tq + 1], cg), f16);
+            bf[1] = pack2(F(ord[k0 + 2 * tq + 8], cg), F(ord[k0 + 2 * tq + 9], cg), f16);
             float d[4] = {F(ra, c0), F(ra, c0 + 1), F(rb, c0), F(rb, c0 + 1)};
             mma16816(d, af, bf, f16);
-            // store rows that are still being updated
-            bool sa = upd_a, sb = upd_b;
-            if (!SPD) {
-              // a row is updated iff it was active after this panel (its final position is >= j1);
-              // positions are known only to the owning lane, so read the active flag via shuffles
-              const int la = ra & 31, lb = rb & 31;
-              const int va = __shfl_sync(kFull, (int)((ra >> 5) == 0 ? act[0] : act[MR - 1]), la);
-              const int vb = __shfl_sync(kFull, (int)((rb >> 5) == 0 ? act[0] : act[MR - 1]), lb);
-              sa = va != 0;
-              sb = vb != 0;
-            }
             if (sa) { F(ra, c0) = d[0]; F(ra, c0 + 1) = d[1]; }
             if (sb) { F(rb, c0) = d[2]; F(rb, c0 + 1) = d[3]; }
           }
         }
       } else {
-        // fp32 CUDA-core update, 4 columns at a time
-        for (int jc = j1; jc < NP; jc += 4) {
+        // fp32 CUDA-core update, 8 columns at a time; each pivot-row segment is read
+        // once for all of a lane's rows
+        for (int jc = j1; jc < NP; jc += 8) {
+          float acc[MR][8];
+#pragma unroll
+          for (int s = 0; s < MR; ++s) {
+            const int r = (lane + 32 * s < NP) ? lane + 32 * s : 0;
+            const float4 a0 = F4(r, jc), a1 = F4(r, jc + 4);
+            acc[s][0] = a0.x; acc[s][1] = a0.y; acc[s][2] = a0.z; acc[s][3] = a0.w;
+            acc[s][4] = a1.x; acc[s][5] = a1.y; acc[s][6] = a1.z; acc[s][7] = a1.w;
+          }
+#pragma unroll
+          for (int i = 0; i < PB; ++i) {
+            float u[8];
+            const float4 v0 = F4(ordp[i], jc), v1 = F4(ordp[i], jc + 4);
+            u[0] = v0.x; u[1] = v0.y; u[2] = v0.z; u[3] = v0.w;
+            u[4] = v1.x; u[5] = v1.y; u[6] = v1.z; u[7] = v1.w;
+#pragma unroll
+            for (int s = 0; s < MR; ++s)
+#pragma unroll
+              for (int q = 0; q < 8; ++q) acc[s][q] = fmaf(-pan[s][i], u[q], acc[s][q]);
+          }
 #pragma unroll
           for (int s = 0; s < MR; ++s) {
             const int r = lane + 32 * s;
-            const bool on = SPD ? (r >= j1 && r < NP) : act[s];
+            const bool on = act[s] && r < NP;
             if (!on) continue;
-            float4 a4 = F4(r, jc);
-            float acc[4] = {a4.x, a4.y, a4.z, a4.w};
-#pragma unroll
-            for (int i = 0; i < PB; ++i) {
-              float u[4];
-              if (SPD) {
-#pragma unroll
-                for (int q = 0; q < 4; ++q) u[q] = F(jc + q, k0 + i);
-              } else {
-                const float4 v = F4(ord[k0 + i], jc);
-                u[0] = v.x; u[1] = v.y; u[2] = v.z; u[3] = v.w;
-              }
-#pragma unroll
-              for (int q = 0; q < 4; ++q) acc[q] = fmaf(-pan[s][i], u[q], acc[q]);
-            }
-            F4(r, jc) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+            F4(r, jc) = make_float4(acc[s][0], acc[s][1], acc[s][2], acc[s][3]);
+            F4(r, jc + 4) = make_float4(acc[s][4], acc[s][5], acc[s][6], acc[s][7]);
           }
         }
       }
       __syncwarp();
     }
     if (p.info && lane == 0) p.info[m] = info;
+    // reciprocal pivots U(ord[k], k)
+#pragma unroll
+    for (int s = 0; s < MR; ++s) {
+      const int k = lane + 32 * s;
+      if (k < NP) rinv[k] = 1.f / F(ord[k], k);
+    }
+    __syncwarp();
 
     // ---------------------------------------- 3./4. solve and refine in fp64
-    // solve(v): v = D_r * rhs (physical rows), returns x = D_c * (U^{-1} L^{-1} P v) into xs
+    // lowsolve(v): v = D_r * rhs by physical row in; the scaled solution by physical row out
     auto lowsolve = [&](float* v) {
       // forward: y_k at physical row ord[k]; rows retired after k take -L(row,k) y_k
       for (int k = 0; k < NP; ++k) {
         const int pk = ord[k];
         float vk = v[0];
-        if (MR > 1 && (pk >> 5) == 1) vk = v[MR - 1];
-        float y = __shfl_sync(kFull, vk, pk & 31);
-        if (SPD) y = y / F(k, k);  // L is not unit-diagonal for Cholesky
+#pragma unroll
+        for (int t2 = 1; t2 < MR; ++t2) vk = ((pk >> 5) == t2) ? v[t2] : vk;
+        const float y = __shfl_sync(kFull, vk, pk & 31);
 #pragma unroll
         for (int s = 0; s < MR; ++s) {
           const int r = lane + 32 * s;
-          const bool after = SPD ? (r > k && r < NP) : (pos[s] > k && r < NP);
-          if (after) v[s] = fmaf(-F(r, k), y, v[s]);
-          if (SPD && r == k) v[s] = y;
+          if (pos[s] > k && r < NP) v[s] = fmaf(-F(r, k), y, v[s]);
         }
       }
-      // backward: x_k = y_k / U(ord[k],k); rows before k take -U(row,k) x_k (SPD: U = L^T)
+      // backward: x_k = y_k / U(ord[k],k); rows retired before k take -U(row,k) x_k
       for (int k = NP - 1; k >= 0; --k) {
         const int pk = ord[k];
         float vk = v[0];
-        if (MR > 1 && (pk >> 5) == 1) vk = v[MR - 1];
-        const float x = __shfl_sync(kFull, vk, pk & 31) / F(pk, k);
+#pragma unroll
+        for (int t2 = 1; t2 < MR; ++t2) vk = ((pk >> 5) == t2) ? v[t2] : vk;
+        const float x = __shfl_sync(kFull, vk, pk & 31) * rinv[k];
 #pragma unroll
         for (int s = 0; s < MR; ++s) {
           const int r = lane + 32 * s;
           if (r == pk) v[s] = x;
-          else {
-            const bool before = SPD ? (r < k) : (pos[s] < k);
-            if (before && r < NP) v[s] = fmaf(-(SPD ? F(k, r) : F(r, k)), x, v[s]);
-          }
+          else if (pos[s] < k && r < NP) v[s] = fmaf(-F(r, k), x, v[s]);
         }
       }
-      // v now holds x by physical row position pk... map to unknown index k: x_k lives at row ord[k]
       __syncwarp();
     };
-    // unknowns: for LU the solution component k sits at physical row ord[k] after the back sweep;
-    // gather into xs[k] (fp64) scaled by the column scale
+    // the solution component of unknown pos[s] sits at physical row r; unscale into xs
     auto gather = [&](const float* v, bool add) {
-      for (int k = lane; k < NP; k += 32) {
-        const int pk = ord[k];
-        (void)pk;
-      }
 #pragma unroll
       for (int s = 0; s < MR; ++s) {
         const int r = lane + 32 * s;
         if (r >= NP) continue;
-        // the row r holds the component of the unknown with position pos (SPD: r)
-        const int kk = SPD ? r : pos[s];
+        const int kk = pos[s];
         const double xk = (double)v[s] * (double)csc[kk];
         if (kk < n) xs[kk] = add ? xs[kk] + xk : xk;
       }
       __syncwarp();
+    };
+    // r = b - A x for the lane's rows lane + 32 s. Rows are read coalesced (lane c
+    // multiplies columns c, c + 32) in chunks of 16; a transposing butterfly folds the
+    // 16 partial sums of each lane so that lanes 2i and 2i + 1 both end with row
+    // 16 ch + i, and one shuffle per chunk hands each row to its owning lane.
+    auto residual = [&](double* rr) {
+      constexpr int NCH = NP / 16;
+      double xl[MR];
+#pragma unroll
+      for (int s = 0; s < MR; ++s) {
+        const int c = lane + 32 * s;
+        xl[s] = (c < n) ? xs[c] : 0.0;
+      }
+      double cv[NCH];
+#pragma unroll
+      for (int ch = 0; ch < NCH; ++ch) {
+        double pp[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int r = 16 * ch + j;
+          double acc = 0.0;
+          if (r < n) {
+            const double* row = Ag + (long long)r * n;
+#pragma unroll
+            for (int s = 0; s < MR; ++s) {
+              const int c = lane + 32 * s;
+              if (c < n) acc = fma(__ldg(row + c), xl[s], acc);
+            }
+          }
+          pp[j] = acc;
+        }
+#pragma unroll
+        for (int o = 16, w = 8; w >= 1; o >>= 1, w >>= 1) {
+          const bool up = (lane & o) != 0;
+#pragma unroll
+          for (int j = 0; j < w; ++j) {
+            const double send = up ? pp[j] : pp[j + w];
+            const double keep = up ? pp[j + w] : pp[j];
+            pp[j] = keep + __shfl_xor_sync(kFull, send, o);
+          }
+        }
+        cv[ch] = pp[0] + __shfl_xor_sync(kFull, pp[0], 1);
+      }
+      // row lane + 32 s is row (lane & 15) of chunk 2 s + (lane >> 4) (chunk 0 only for NP = 16)
+#pragma unroll
+      for (int s = 0; s < MR; ++s) {
+        const int r = lane + 32 * s;
+        const double a = __shfl_sync(kFull, cv[(2 * s) < NCH ? 2 * s : NCH - 1], 2 * (lane & 15));
+        const double b = __shfl_sync(kFull, cv[(2 * s + 1) < NCH ? 2 * s + 1 : NCH - 1], 2 * (lane & 15));
+        const double sum = (lane >> 4) ? b : a;
+        rr[s] = (r < n) ? bv[s] - sum : 0.0;
+      }
     };
     float v[MR];
 #pragma unroll
@@ -451,21 +504,15 @@ __global__ void __launch_bounds__(WPC * 32, 1) ir_kernel(IrArgs p) {
     double be = 1.0, be_prev = 1e300;
     bool conv = false;
     for (int it = 0; it <= p.itmax + 1; ++it) {
-      // r = b - A x, lane r owns rows r, r + 32
       double rr[MR];
+      residual(rr);
       double rn = 0.0, xn = 0.0;
 #pragma unroll
       for (int s = 0; s < MR; ++s) {
-        const int r = lane + 32 * s;
-        double acc = bv[s];
-        if (r < n) {
-          const double* row = Ag + (long long)r * n;
-          for (int c = 0; c < n; ++c) acc = fma(-row[c], xs[c], acc);
-        }
-        rr[s] = (r < n) ? acc : 0.0;
         rn = fma(rr[s], rr[s], rn);
+        const int c = lane + 32 * s;
+        if (c < n) xn = fma(xs[c], xs[c], xn);
       }
-      for (int c = lane; c < n; c += 32) xn = fma(xs[c], xs[c], xn);
       for (int o = 16; o > 0; o >>= 1) {
         rn += __shfl_xor_sync(kFull, rn, o);
         xn += __shfl_xor_sync(kFull, xn, o);

@@ -12,8 +12,11 @@ namespace host {
 template <int NP, bool SPD>
 int launch_ir(const dev::IrArgs& a, cudaStream_t st) {
   using C = dev::IrCfg<NP>;
+  // at most 12 warps from order 32 up: 170 registers per thread keep the panel,
+  // the trailing-update accumulators and the residual butterfly out of local memory
   constexpr int FIT = (227 * 1024) / C::WARPB;
-  constexpr int WPC = FIT < 1 ? 1 : (FIT > 16 ? 16 : FIT);
+  constexpr int CAP = NP >= 32 ? 12 : 16;
+  constexpr int WPC = FIT < 1 ? 1 : (FIT > CAP ? CAP : FIT);
   constexpr int SMEM = WPC * C::WARPB;
   auto kern = dev::ir_kernel<NP, SPD, WPC>;
   if (int rc = prepare(kern, SMEM)) return rc;
