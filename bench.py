@@ -2,12 +2,19 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
-A step is one pass of the hot path over one batch: plain LU with partial
-pivoting plus the solve (gesv: A <- L\\U, B <- X, pivots, info) in float64 on
-(65,536 x 64 x 64) general matrices with 4 right-hand sides, kappa log-uniform
-in [1e1, 1e8] and 5% of the matrices with one zeroed column (the n=64 case of
-the plain-LU benchmark configuration). Inputs are synthetic, built on the
-device with the reference's generator construction, and larger than L2.
+A step is one pass of the hot path over one batch. The default workload is
+plain LU with partial pivoting plus the solve (gesv: A <- L\\U, B <- X, pivots,
+info) in float64 on (65,536 x 64 x 64) general matrices with 4 right-hand sides,
+kappa log-uniform in [1e1, 1e8] and 5% of the matrices with one zeroed column
+(the n=64 case of the plain-LU benchmark configuration). Other workloads
+(--workload): the n=32 / float32 variants and Cholesky n=16; ``ir_n64``, the
+mixed-precision solve with per-matrix tiers from the learned selector and fp64
+refinement (131,072 matrices, half SPD, kappa up to 1e12), next to plain fp64 on
+the same inputs; ``stream_f32``, the uneven stream (1,048,576 matrices of mixed
+order, kind and right-hand-side count in one graph-captured launch sequence); and
+``selector``, the selector's evaluation set (1,048,576 matrices, n 8..64, kappa up
+to 1e14) against fixed-tier policies and plain fp64. Inputs are synthetic, built
+on the device with the reference's generator construction, and larger than L2.
 
 The ours arm prints one JSON line: device-resident throughput (value), the
 end-to-end throughput of the host-pointer C-ABI call with pinned host buffers
@@ -41,6 +48,15 @@ WORKLOADS = {
     "gesv_f32_n64": ("gesv", 64, 65536, 4, "f32", 1e1, 1e8, 0.05),
     "gesv_f32_n32": ("gesv", 32, 262144, 4, "f32", 1e1, 1e8, 0.05),
     "posv_f64_n16": ("posv", 16, 65536, 1, "f64", 1e1, 1e6, 0.0),
+}
+SPECIAL = {
+    "ir_n64": "mixed precision (selector-chosen fp16/bf16/fp32/fp64 tier per matrix) + fp64 iterative "
+              "refinement with fp64 fallback, n=64, batch 131,072 (half SPD Cholesky, half general LU), "
+              "1 RHS, kappa log-uniform [1e1,1e12]",
+    "stream_f32": "uneven stream, fp32, 1,048,576 matrices, n uniform {2..64}, 50% SPD Cholesky / 50% LU, "
+                  "kappa log-uniform [1e1,1e8], RHS count uniform {1,2,4,8}, one graph-captured launch sequence",
+    "selector": "learned tier selector evaluation: 1,048,576 matrices, n uniform {8..64}, half SPD / half LU, "
+                "kappa log-uniform [1e0,1e14], 1 RHS, selector tiers + fp64 refinement + fp64 fallback",
 }
 
 
@@ -302,7 +318,7 @@ def run_ours(a):
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": src,
             "algorithmic_bytes_per_launch": per_launch,
-            "kernel": ("lu_blk_kernel" if kind == "gesv" else "chol_team_kernel") + f"<{dt},NP={n}>",
+            "kernel": f"blk_kernel<{dt},NP={n},{'LU' if kind == 'gesv' else 'Cholesky'}>",
             "gflops": round(batch * flops(kind, n, nrhs) / (ms_step * 1e-3) / 1e9, 1)}
 
     cpu = None
@@ -349,13 +365,498 @@ def run_reference(a):
     print(json.dumps(out), flush=True)
 
 
+
+# ---------------------------------------------------------------- mixed precision, stream, selector
+def _pkg(sub):
+    return importlib.import_module(PKG_NAME + "." + sub)
+
+
+def _dist_setup():
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
+    return world, rank, local, device, dist
+
+
+def _max_over_ranks(ms, world, device, dist):
+    import torch
+    if world > 1:
+        t = torch.tensor([ms], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms
+
+
+def _timed(step, a, world, local, device, dist):
+    """W untimed steps, then K steps between barriers + syncs, CUDA events on the
+    launching stream; returns (ms per step (max over ranks), clocks, launches)."""
+    import torch
+    capi = _pkg("capi")
+    for i in range(a.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    l0 = capi.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(st)
+        for i in range(a.steps):
+            step(a.warmup + i)
+        e1.record(st)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = _max_over_ranks(e0.elapsed_time(e1) / a.steps, world, device, dist)
+    return ms, clk.summary(), capi.launch_count() - l0
+
+
+def _once(fn):
+    """Device time of one call (ms), synchronized on both sides."""
+    import torch
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def _bwd(A, x, b):
+    """Normwise backward error ||b - A x||_2 / (||A||_F ||x||_2 + ||b||_2) per matrix, fp64 on the device."""
+    import torch
+    r = b - torch.bmm(A, x.unsqueeze(-1))[..., 0]
+    return r.norm(dim=1) / (A.flatten(1).norm(dim=1) * x.norm(dim=1) + b.norm(dim=1))
+
+
+def _stats(v):
+    import torch
+    v = v.double()
+    return {"median": float(v.median().item()), "max": float(v.max().item())}
+
+
+def _threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def _cpu_solves(groups, budget_s=12.0):
+    """Reference CPU (compiled from its sources, else the C restatement), all host
+    threads, on host samples: groups = [(kind, A (b,n,n), B (b,n,r))]. Returns
+    (solves/s, threads, kind)."""
+    from oracle.oracle import Oracle, ref_available
+    kindlib = "reference" if ref_available() else "port"
+    O = Oracle(kindlib)
+    thr = _threads()
+    O.set_num_threads(thr)
+    best, total, reps = 0.0, 0.0, 0
+    count = sum(g[1].shape[0] for g in groups)
+    while total < budget_s and reps < 20:
+        work = [(k, A.copy(), B.copy()) for k, A, B in groups]
+        t0 = time.perf_counter()
+        for k, A, B in work:
+            b, n, r = B.shape
+            s = "d" if A.dtype == np.float64 else "f"
+            info = np.zeros(b, np.int32)
+            if kindlib == "reference":
+                if k == "gesv":
+                    piv = np.zeros((b, n), np.int32)
+                    getattr(O.lib, f"ref_gesv_batched_{s}")(A.ctypes.data_as(C.c_void_p), n, b,
+                                                            B.ctypes.data_as(C.c_void_p), r,
+                                                            piv.ctypes.data_as(C.c_void_p),
+                                                            info.ctypes.data_as(C.c_void_p), 0)
+                else:
+                    getattr(O.lib, f"ref_posv_batched_{s}")(A.ctypes.data_as(C.c_void_p), n, b,
+                                                            B.ctypes.data_as(C.c_void_p), r,
+                                                            info.ctypes.data_as(C.c_void_p), 0)
+            else:
+                (O.gesv if k == "gesv" else O.posv)(A, B)
+        dt = time.perf_counter() - t0
+        total += dt
+        reps += 1
+        best = max(best, count / dt)
+    return best, thr, kindlib
+
+
+def _emit(a, world, value, ms, dt, cfg, roof, cpu, e2e, clk, launches, extra=None, impl=None):
+    out = {"metric": METRIC, "value": round(value, 1), "unit": "solves/s", "n_gpus": world, "steps": a.steps,
+           "warmup": a.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": dt, "data": "synthetic", "config": cfg}
+    if impl:
+        out["impl"] = impl
+    if roof is not None:
+        out["roofline"] = roof
+    out["cpu_baseline"] = cpu
+    out["e2e"] = e2e
+    if clk is not None:
+        out["clocks"] = clk
+    if launches is not None:
+        out["gpu_launches"] = int(launches)
+    if extra:
+        out.update(extra)
+    print(json.dumps(out), flush=True)
+
+
+def _roof(bytes_per_step, ms, kernel, flops_per_step=None, traffic=None):
+    peak, src = peaks()
+    ach = bytes_per_step / (ms * 1e-3) / 1e9
+    r = {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
+         "traffic": traffic, "peak_source": src, "algorithmic_bytes_per_launch": int(bytes_per_step),
+         "kernel": kernel}
+    if flops_per_step:
+        r["gflops"] = round(flops_per_step / (ms * 1e-3) / 1e9, 1)
+    return r
+
+
+def _selector(device):
+    sel = _pkg("selector")
+    w = ROOT / PKG_NAME / "selector_weights.npz"
+    if not w.exists():
+        raise RuntimeError(f"{w} is missing: train it with {PKG_NAME}/selector_train.py")
+    return sel.Selector.load(str(w), device=device)
+
+
+def _ir_workload(a, world, rank, local, device, dist):
+    import torch
+    M, sel, dev = _pkg("matrices"), _pkg("selector"), _pkg("device")
+    n = 64
+    batch = a.batch or 131072
+    half = batch // 2
+    parts = []
+    for spd, cnt, seed in ((True, half, 4321 + rank), (False, batch - half, 8765 + rank)):
+        A = M.torch_stack("spd" if spd else "general", n, cnt, 1e1, 1e12, seed, device=device).contiguous()
+        g = torch.Generator(device=device)
+        g.manual_seed(seed + 1)
+        parts.append((spd, A, torch.randn(cnt, n, generator=g, device=device, dtype=torch.float64)))
+    s = _selector(device)
+    pool = max(2, min(a.steps + a.warmup, 24))
+    xs = [[b.clone() for _ in range(pool)] for _, _, b in parts]
+
+    def step(i):
+        for (spd, A, _), bp in zip(parts, xs):
+            s.solve(A, bp[i % pool], spd)
+
+    ms, clk, launches = _timed(step, a, world, local, device, dist)
+    value = world * batch / (ms * 1e-3)
+    # the same inputs through plain fp64 (x only, A untouched) and fixed-tier policies, one pass each
+    extra, tiers, bw = {}, {}, {}
+    for name, tier in (("plain_fp64", 3), ("fixed_fp32", 2), ("fixed_bf16", 1), ("fixed_fp16", 0)):
+        t = 0.0
+        fall = 0
+        for spd, A, b in parts:
+            x = b.clone()
+            res = {}
+
+            def run():
+                res["st"] = dev.ir(A, x, spd, default_tier=tier)[1]
+            t += _once(run)
+            if tier < 3:
+                fall += int((res["st"] < 0).sum().item())
+            if name == "plain_fp64":
+                bw.setdefault("plain_fp64", []).append(_bwd(A, x, b))
+        extra[name] = {"solves_per_s": round(batch / (t * 1e-3), 1), "ms": round(t, 4)}
+        if tier < 3:
+            extra[name]["fp64_fallbacks"] = fall
+    for spd, A, b in parts:
+        x = b.clone()
+        info, status, bwd, tier = s.solve(A, x, spd)
+        be = _bwd(A, x, b)
+        bw.setdefault("selector", []).append(be)
+        for t in range(4):
+            sel_t = (tier == t)
+            tiers[sel.TIERS[t]] = tiers.get(sel.TIERS[t], 0) + int(sel_t.sum().item())
+            ok = sel_t & (status >= 0)
+            if ok.any():
+                bw.setdefault(f"refined_{sel.TIERS[t]}", []).append(be[ok])
+        tiers["fp64_fallbacks"] = tiers.get("fp64_fallbacks", 0) + int(((tier < 3) & (status < 0)).sum().item())
+    errs = {k: _stats(torch.cat(v)) for k, v in bw.items()}
+    extra["selector_tiers"] = tiers
+    extra["backward_error"] = errs
+    extra["bwd_max_ratio_vs_plain_fp64"] = round(errs["selector"]["max"] / errs["plain_fp64"]["max"], 3)
+    extra["speedup_vs_plain_fp64"] = round(value / world / extra["plain_fp64"]["solves_per_s"], 3)
+    bytes_step = batch * (8 * (n * n + 2 * n) + 4)
+    roof = _roof(bytes_step, ms, "ir_kernel<64> (+ features, mlp_forward, fp64 fallback blk_kernel)",
+                 traffic=traffic_from_profiles("ir_n64"))
+    # end to end: pinned host A and b in, x and info out, every step
+    e2e = None
+    if not a.skip_e2e:
+        hp = [(spd, A.cpu().pin_memory(), b.cpu().pin_memory()) for spd, A, b in parts]
+        dA = [torch.empty_like(A) for _, A, _ in parts]
+        dx = [torch.empty_like(b) for _, _, b in parts]
+        hx = [torch.empty(b.shape, dtype=b.dtype, pin_memory=True) for _, _, b in parts]
+        hi = [torch.empty(b.shape[0], dtype=torch.int32, pin_memory=True) for _, _, b in parts]
+
+        def e2e_step():
+            for (spd, hA, hb), A_, x_, hx_, hi_ in zip(hp, dA, dx, hx, hi):
+                A_.copy_(hA, non_blocking=True)
+                x_.copy_(hb, non_blocking=True)
+                info, _, _, _ = s.solve(A_, x_, spd)
+                hx_.copy_(x_, non_blocking=True)
+                hi_.copy_(info, non_blocking=True)
+        e2e_step()
+        t = min(_once(e2e_step) for _ in range(3))
+        t = _max_over_ranks(t, world, device, dist)
+        e2e = {"value": round(world * batch / (t * 1e-3), 1), "unit": "solves/s",
+               "h2d_bytes_per_step": batch * (n * n + n) * 8, "d2h_bytes_per_step": batch * (n * 8 + 4),
+               "ms_per_step": round(t, 3), "api": "Selector.solve (features + tier + tsdx_cuda_*_ir_f64), pinned host"}
+    cpu = None
+    if rank == 0 and world == 1 and not a.skip_cpu:
+        rng = np.random.default_rng(5)
+        smp = 2048
+        kap = M.log_uniform(rng, smp, 1e1, 1e12)
+        groups = [("posv", M.spd(rng, smp, n, kap), rng.standard_normal((smp, n, 1))),
+                  ("gesv", M.general(rng, smp, n, kap), rng.standard_normal((smp, n, 1)))]
+        v, thr, kl = _cpu_solves(groups)
+        cpu = {"value": round(v, 1), "unit": "solves/s", "cores": thr, "kind": kl,
+               "sample": f"{2 * smp} n=64 fp64 solves (half posv, half gesv), 1 RHS, per call best of repeated calls"}
+    cfg = {"workload": SPECIAL["ir_n64"], "global_batch": world * batch, "batch_per_gpu": batch,
+           "parallelism": f"batch sharded over {world} GPU(s), no collective",
+           "l2": "inputs larger than L2 (4.3 GB of A per step)",
+           "selector": f"{PKG_NAME}/selector_weights.npz"}
+    return value, ms, "f64 (tiers fp16/bf16/fp32 factor, fp64 residual)", cfg, roof, cpu, e2e, clk, launches, extra
+
+
+def _stream_workload(a, world, rank, local, device, dist):
+    import torch
+    M, stream = _pkg("matrices"), _pkg("stream")
+    count = a.batch or 1048576
+    g = np.random.default_rng(1000 + rank)
+    n = g.integers(2, 65, count).astype(np.int32)
+    kind = g.integers(0, 2, count).astype(np.int8)
+    nrhs = g.choice([1, 2, 4, 8], count).astype(np.int32)
+    aoff, boff, poff, na, nb, npv = stream.layout(n, nrhs)
+    A0 = torch.empty(na, dtype=torch.float32, device=device)
+    key = kind.astype(np.int64) * 100 + n
+    order = np.argsort(key, kind="stable")
+    ks, starts = np.unique(key[order], return_index=True)
+    starts = list(starts) + [count]
+    aoff_d = aoff.to(device)
+    for gi, k in enumerate(ks):
+        idx = order[starts[gi]:starts[gi + 1]]
+        nn, kk = int(k % 100), int(k // 100)
+        X = M.torch_stack("spd" if kk == 0 else "general", nn, len(idx), 1e1, 1e8, 2000 + gi + 97 * rank,
+                          device=device).float()
+        dst = aoff_d[torch.from_numpy(idx).to(device)][:, None] + torch.arange(nn * nn, device=device)[None, :]
+        A0[dst.reshape(-1)] = X.reshape(-1)
+        del X, dst
+    gB = torch.Generator(device=device)
+    gB.manual_seed(3000 + rank)
+    B0 = torch.randn(nb, generator=gB, dtype=torch.float32, device=device)
+    plan = stream.StreamPlan(n, nrhs, kind, torch.float32, device=device)
+    plan.tune(A0, B0, reps=2)
+    pool = max(2, min(a.steps + a.warmup, 11))
+    As = [A0.clone() for _ in range(pool)]
+    Bs = [B0.clone() for _ in range(pool)]
+    graphs = []
+    for j in range(pool):
+        gr = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(gr):
+            stream.solve(As[j], plan.aoff, Bs[j], plan.boff, plan.piv, plan.poff, plan.info, plan.n, plan.nrhs,
+                         plan.kind, True, plan.sched, plan.scratch)
+        graphs.append(gr)
+    # reset the pool after the captures' side effects (capture does not run kernels, but be explicit)
+    for j in range(pool):
+        As[j].copy_(A0)
+        Bs[j].copy_(B0)
+    capi = _pkg("capi")
+    ms, clk, _ = _timed(lambda i: graphs[i % pool].replay(), a, world, local, device, dist)
+    launches = 4 * a.steps  # memset + histogram, scan, scatter, drain per replay (counted at capture)
+    value = world * count / (ms * 1e-3)
+    n64 = n.astype(np.int64)
+    bytes_step = int((4 * (2 * n64 * n64 + 2 * n64 * nrhs) + 4 + np.where(kind == 1, 4 * n64, 0)).sum())
+    flops_step = float((np.where(kind == 1, 2 * n64 ** 3 / 3, n64 ** 3 / 3) + 2 * n64 * n64 * nrhs).sum())
+    roof = _roof(bytes_step, ms, "stream_kernel<float> (+ histogram, scan, scatter)", flops_step,
+                 traffic_from_profiles("stream_f32"))
+    extra = {"schedule": {"sched_bits": plan.sched, "tuned_ms": {str(k): round(v, 3) for k, v in plan.timings.items()}}}
+    e2e = None
+    if not a.skip_e2e:
+        hA, hB = A0.cpu().pin_memory(), B0.cpu().pin_memory()
+        oA = torch.empty_like(hA).pin_memory()
+        oB = torch.empty_like(hB).pin_memory()
+        oP = torch.empty(plan.piv.shape, dtype=torch.int32).pin_memory()
+        oI = torch.empty(plan.info.shape, dtype=torch.int32).pin_memory()
+        plan.capture()
+
+        def e2e_step():
+            plan.A.copy_(hA, non_blocking=True)
+            plan.B.copy_(hB, non_blocking=True)
+            plan.run()
+            oA.copy_(plan.A, non_blocking=True)
+            oB.copy_(plan.B, non_blocking=True)
+            oP.copy_(plan.piv, non_blocking=True)
+            oI.copy_(plan.info, non_blocking=True)
+        e2e_step()
+        t = _max_over_ranks(min(_once(e2e_step) for _ in range(3)), world, device, dist)
+        e2e = {"value": round(world * count / (t * 1e-3), 1), "unit": "solves/s",
+               "h2d_bytes_per_step": (na + nb) * 4, "d2h_bytes_per_step": (na + nb + npv + count) * 4,
+               "ms_per_step": round(t, 3), "api": "stream.StreamPlan (tsdx_cuda_solve_stream_f32), pinned host"}
+    cpu = None
+    if rank == 0 and world == 1 and not a.skip_cpu:
+        smp = 16384
+        groups = {}
+        A_h = A0[:int(aoff[smp])].cpu().numpy() if smp < count else A0.cpu().numpy()
+        B_h = B0[:int(boff[smp])].cpu().numpy() if smp < count else B0.cpu().numpy()
+        for i in range(min(smp, count)):
+            ni, ri = int(n[i]), int(nrhs[i])
+            groups.setdefault((int(kind[i]), ni, ri), []).append(i)
+        cg = []
+        for (k, ni, ri), idx in groups.items():
+            As_ = np.stack([A_h[int(aoff[i]):int(aoff[i]) + ni * ni].reshape(ni, ni) for i in idx])
+            Bs_ = np.stack([B_h[int(boff[i]):int(boff[i]) + ni * ri].reshape(ni, ri) for i in idx])
+            cg.append(("gesv" if k else "posv", As_, Bs_))
+        v, thr, kl = _cpu_solves(cg)
+        cpu = {"value": round(v, 1), "unit": "solves/s", "cores": thr, "kind": kl,
+               "sample": f"first {min(smp, count)} matrices of the stream, one reference call per (kind, n, nrhs) "
+                         f"group ({len(cg)} groups), summed"}
+    cfg = {"workload": SPECIAL["stream_f32"], "global_batch": world * count, "batch_per_gpu": count,
+           "parallelism": f"stream sharded over {world} GPU(s), no collective",
+           "l2": f"inputs larger than L2 ({na * 4 / 1e9:.1f} GB of A), {pool} input copies cycled"}
+    return value, ms, "f32", cfg, roof, cpu, e2e, clk, launches, extra
+
+
+def _selector_workload(a, world, rank, local, device, dist):
+    import torch
+    sel, dev, M = _pkg("selector"), _pkg("device"), _pkg("matrices")
+    train = importlib.import_module(PKG_NAME + ".selector_train")
+    count = a.batch or 1048576
+    X, y, groups = train.dataset(count, 77 + rank, device=device, keep=True)
+    s = _selector(device)
+    pred = s.predict(X)
+    acc = float((pred == y).float().mean().item())
+    confusion = torch.zeros(4, 4, dtype=torch.int64)
+    for t in range(4):
+        for p_ in range(4):
+            confusion[t, p_] = int(((y == t) & (pred == p_)).sum().item())
+    pool = 2
+
+    def step(i):
+        for gr in groups:
+            s.solve(gr["A"], gr["xs"][i % pool], gr["spd"])
+
+    for gr in groups:
+        gr["xs"] = [gr["b"].clone() for _ in range(pool)]
+    ms, clk, launches = _timed(step, a, world, local, device, dist)
+    value = world * count / (ms * 1e-3)
+    extra = {"label_accuracy": round(acc, 4), "confusion_true_by_pred": confusion.tolist(),
+             "label_counts": dict(zip(sel.TIERS, torch.bincount(y.long(), minlength=4).cpu().tolist()))}
+    # policies without the network, and a perfect selector (the labels), one pass each
+    policies = {"plain_fp64": 3, "fixed_fp32": 2, "fixed_fp16": 0, "oracle_labels": None}
+    bw = {}
+    off = 0
+    for name, tier in policies.items():
+        t, fall = 0.0, 0
+        for gr in groups:
+            x = gr["b"].clone()
+            res = {}
+            tt = None if tier is not None else s.policy(gr["y"], gr["n"], gr["spd"]).to(torch.int8).contiguous()
+
+            def run():
+                res["st"] = dev.ir(gr["A"], x, gr["spd"], tier=tt, default_tier=3 if tier is None else tier)[1]
+            t += _once(run)
+            if tier != 3:
+                fall += int(((res["st"] < 0) & ((tt < 3) if tier is None else True)).sum().item())
+            if name == "plain_fp64":
+                bw.setdefault("plain_fp64", []).append(_bwd(gr["A"], x, gr["b"]))
+        extra[name] = {"solves_per_s": round(count / (t * 1e-3), 1), "ms": round(t, 3)}
+        if tier != 3:
+            extra[name]["fp64_fallbacks"] = fall
+    fall = 0
+    for gr in groups:
+        x = gr["b"].clone()
+        _, status, _, tier = s.solve(gr["A"], x, gr["spd"])
+        bw.setdefault("selector", []).append(_bwd(gr["A"], x, gr["b"]))
+        fall += int(((tier < 3) & (status < 0)).sum().item())
+    extra["selector_fp64_fallbacks"] = fall
+    errs = {k: _stats(torch.cat(v)) for k, v in bw.items()}
+    extra["backward_error"] = errs
+    extra["speedup_vs_plain_fp64"] = round(value / world / extra["plain_fp64"]["solves_per_s"], 3)
+    extra["speedup_vs_fixed_fp16"] = round(value / world / extra["fixed_fp16"]["solves_per_s"], 3)
+    extra["speedup_vs_fixed_fp32"] = round(value / world / extra["fixed_fp32"]["solves_per_s"], 3)
+    nsum = sum(gr["count"] * (8 * (gr["n"] ** 2 + 2 * gr["n"]) + 4) for gr in groups)
+    roof = _roof(nsum, ms, "ir_kernel (+ features, mlp_forward, fp64 fallback)", traffic=None)
+    cfg = {"workload": SPECIAL["selector"], "global_batch": world * count, "batch_per_gpu": count,
+           "parallelism": f"evaluation set sharded over {world} GPU(s), no collective",
+           "l2": "inputs larger than L2 (13 GB of A per step)", "selector": f"{PKG_NAME}/selector_weights.npz"}
+    return value, ms, "f64 (tiers fp16/bf16/fp32 factor, fp64 residual)", cfg, roof, None, None, clk, launches, extra
+
+
+def run_ours_special(a):
+    world, rank, local, device, dist = _dist_setup()
+    fn = {"ir_n64": _ir_workload, "stream_f32": _stream_workload, "selector": _selector_workload}[a.workload]
+    value, ms, dt, cfg, roof, cpu, e2e, clk, launches, extra = fn(a, world, rank, local, device, dist)
+    if rank == 0:
+        _emit(a, world, value, ms, dt, cfg, roof, cpu, e2e, clk, launches, extra)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_reference_special(a):
+    """The reference's own CPU implementation on a bounded sample of the workload:
+    plain fp64 posv/gesv for the mixed-precision workloads (the reference has no
+    mixed-precision path), per-(kind, n, nrhs) group calls for the stream."""
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    M = _pkg("matrices")
+    vals = []
+    budget = max(2.0, 150.0 / max(1, a.steps + a.warmup))
+    rng = np.random.default_rng(9)
+    if a.workload == "stream_f32":
+        groups = []
+        for kk in (0, 1):
+            for ni in range(2, 65):
+                for r in (1, 2, 4, 8):
+                    kap = M.log_uniform(rng, 16, 1e1, 1e8)
+                    A = (M.spd if kk == 0 else M.general)(rng, 16, ni, kap).astype(np.float32)
+                    groups.append(("posv" if kk == 0 else "gesv", A,
+                                   rng.standard_normal((16, ni, r)).astype(np.float32)))
+        sample = "16 fp32 matrices per (kind, n, nrhs) for every n in 2..64, both kinds, nrhs in {1,2,4,8} (8064)"
+    else:
+        sizes = (64,) if a.workload == "ir_n64" else (8, 24, 40, 56, 64)
+        khi = 1e12 if a.workload == "ir_n64" else 1e14
+        groups = []
+        for ni in sizes:
+            for kk in ("posv", "gesv"):
+                kap = M.log_uniform(rng, 1024, 1e1, khi)
+                A = (M.spd if kk == "posv" else M.general)(rng, 1024, ni, kap)
+                groups.append((kk, A, rng.standard_normal((1024, ni, 1))))
+        sample = f"1024 fp64 matrices per (kind, n) for n in {sizes}, 1 RHS, plain posv/gesv"
+    thr, kl = 1, "port"
+    for i in range(a.warmup + a.steps):
+        v, thr, kl = _cpu_solves(groups, budget_s=budget)
+        if i >= a.warmup:
+            vals.append(v)
+    value = float(np.median(vals))
+    cfg = {"workload": SPECIAL[a.workload]}
+    per_step = {"ir_n64": 131072, "stream_f32": 1048576, "selector": 1048576}[a.workload]
+    cfg["global_batch"] = per_step
+    _emit(a, world, value, per_step / value * 1e3, "f32" if a.workload == "stream_f32" else "f64", cfg, None,
+          {"value": round(value, 1), "unit": "solves/s", "cores": thr, "kind": kl, "sample": sample},
+          {"value": round(value, 1), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+          None, None, impl="reference")
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="gesv_f64_n64", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="gesv_f64_n64", choices=sorted(WORKLOADS) + sorted(SPECIAL))
     ap.add_argument("--batch", type=int, default=0, help="override the workload's batch (profiling runs)")
     ap.add_argument("--pool", type=int, default=12, help="distinct input copies cycled through the steps")
     ap.add_argument("--skip-e2e", action="store_true")
@@ -364,9 +865,9 @@ def main(argv=None):
     if a.warmup < 3:
         a.warmup = 3
     if a.impl == "reference":
-        run_reference(a)
+        (run_reference_special if a.workload in SPECIAL else run_reference)(a)
     else:
-        run_ours(a)
+        (run_ours_special if a.workload in SPECIAL else run_ours)(a)
 
 
 if __name__ == "__main__":

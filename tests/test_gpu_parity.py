@@ -197,7 +197,7 @@ def test_golden_vectors(golden):
 
 @pytest.mark.parametrize("n,batch", [(4, 200_003), (16, 70_001), (64, 5_001)])
 def test_large_batch_loops(oracle, n, batch):
-    """Batches larger than one wave of resident teams exercise the persistent loop."""
+    """Batches larger than one wave of resident warps exercise the persistent loop."""
     rng = np.random.default_rng(n)
     A = rng.standard_normal((batch, n, n))
     LU, piv, info = gpu_getrf(A)
@@ -273,7 +273,7 @@ def test_argument_errors():
 
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
 def test_markstein_division(dtype):
-    """div_by (shared reciprocal + Markstein correction, team.cuh) equals IEEE division bit for bit."""
+    """div_by (shared reciprocal + Markstein correction, common.cuh) equals IEEE division bit for bit."""
     rng = np.random.default_rng(17)
     m = 4_000_000
     lo, hi = (-300, 300) if dtype == np.float64 else (-35, 35)

@@ -29,7 +29,7 @@
 // The per-matrix body is a device function over a MatJob (base pointers, sizes),
 // shared by the dense-batch kernel below and the uneven-stream kernel.
 #pragma once
-#include "team.cuh"
+#include "common.cuh"
 
 namespace tsdx {
 namespace dev {

@@ -230,7 +230,7 @@ API int tsdx_cuda_available(void) {
 API const char* tsdx_cuda_last_error(void) { return tsdx::host::g_err.c_str(); }
 API int64_t tsdx_cuda_launch_count(void) { return tsdx::host::launch_counter().load(); }
 
-// Self-check of the Markstein-corrected division used by the kernels (team.cuh
+// Self-check of the Markstein-corrected division used by the kernels (common.cuh
 // div_by) against the IEEE division, element by element. Not part of the solver
 // API; the test-suite calls it on adversarial operand sets.
 namespace {

@@ -1,29 +1,16 @@
-// Register-resident "team" kernels for batched small-matrix Cholesky / LU on sm_100a.
+// Shared device helpers of the batched small-matrix kernels (sm_100a): argument
+// block, element-type traits, the bit-exact arithmetic building blocks, and copy
+// helpers.
 //
-// One team of TW warps owns one matrix (TW == 1 and n <= 16: one warp owns 32/G
-// matrices, G lanes each). Lane l of a team owns matrix rows {l + G*s}; with
-// TW > 1 the columns are dealt to the warps in groups of 16 bytes. The whole
-// matrix plus its right-hand sides (the augmented columns NP..NP+NRHS-1) lives in
-// registers for the entire factorization, so the rank-1 trailing update never
-// touches shared memory; shared memory only carries the per-step broadcasts (the
-// pivot row, the Cholesky column, the multipliers when TW > 1) and the coalesced
-// staging of the global loads and stores.
-//
-// Bit-exactness. Each element receives exactly the reference's chain of
+// Bit-exactness. Every factor element receives exactly the reference's chain of
 // operations (TinySolverDx kernels.hpp): LU (kernels.hpp:91-119) a_ij <-
-// fma(-l_ik, u_kj, a_ij) in increasing k with l_ik = a_ik / u_kk an IEEE
-// division; Cholesky as the reference's default simd backend compiles it
-// (kernels.hpp:57-87: fused for n <= 16, separately rounded product and
-// subtraction for n >= 17). The forward substitution is fused into the
-// elimination as extra columns, which is the same chain as kernels.hpp:184-193 /
-// 214-218. Pivoting is implicit: rows never move, a position table replays the
-// reference's row swaps so its tie-breaking (strict '>', first maximum wins, NaN
-// never wins unless it sits on the diagonal position) is reproduced exactly, and
-// each row is written out at the position where it was retired, which is exactly
-// where the reference's full-row swaps leave it.
-//
-// The back substitution is column-oriented (decreasing k), so X agrees with the
-// reference to rounding (backward error within c*n*u), not bit-for-bit.
+// fma(-l_ik, u_kj, a_ij) in increasing k with l_ik = a_ik / u_kk correctly
+// rounded (Markstein-corrected reciprocal below); Cholesky as the reference's
+// default simd backend compiles it (kernels.hpp:57-87: fused for n <= 16, product
+// rounded before the subtraction for n >= 17, sub_mul below). The pivot search
+// compares keys built from |a| so that the reference's tie-breaking (strict '>',
+// first maximum wins, NaN never wins unless it sits on the diagonal position) is
+// reproduced exactly (seg_argmax below).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -116,30 +103,6 @@ struct FastDiv {
   __host__ __device__ FastDiv() : d(1), m(0) {}
   __host__ __device__ explicit FastDiv(unsigned dd) : d(dd), m((unsigned)((0x100000000ull + dd - 1) / dd)) {}
   __device__ __forceinline__ unsigned div(unsigned x) const { return d == 1 ? x : __umulhi(x, m); }
-};
-
-// ---- layout -------------------------------------------------------------------
-template <class T, int NP, int NRHS, int TW>
-struct Layout {
-  static constexpr int G = (TW > 1 || NP > 16) ? 32 : NP <= 4 ? 4 : NP <= 8 ? 8 : 16;  // lanes per matrix
-  static constexpr int S = (TW == 1) ? 32 / G : 1;                                        // matrices per warp
-  static constexpr int MR = (NP + G - 1) / G;                                             // row slots per lane
-  static constexpr int NC = NP + NRHS;                                                    // augmented columns
-  static constexpr int CW = (TW == 1) ? 1 : int(16 / sizeof(T));                         // column group width
-  static constexpr int NGRP = (NC + CW - 1) / CW;
-  static constexpr int MC = (TW == 1) ? NC : ((NGRP + TW - 1) / TW) * CW;                 // column slots per warp
-  static constexpr int RS = NP * int(sizeof(T)) + 16;                                     // padded staging row (bytes)
-  static constexpr int BUF = NP * RS;                                                     // staging bytes per matrix
-  static_assert(NP % 4 == 0, "NP must be a multiple of 4");
-  static_assert(TW == 1 || (NP / CW) % TW == 0, "B columns must start a column group");
-  static_assert(MR <= 2, "at most two row slots per lane");
-  __host__ __device__ static constexpr int col(int w, int c) {
-    return TW == 1 ? c : ((c / CW) * TW + w) * CW + (c % CW);
-  }
-  __host__ __device__ static constexpr int cmin(int c) { return col(0, c); }
-  __host__ __device__ static constexpr int cmax(int c) { return col(TW - 1, c); }
-  __host__ __device__ static constexpr int owner(int j) { return TW == 1 ? 0 : (j / CW) % TW; }
-  __host__ __device__ static constexpr int slot(int j) { return TW == 1 ? j : ((j / CW) / TW) * CW + (j % CW); }
 };
 
 template <class T>

@@ -25,7 +25,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
-#include "team.cuh"
+#include "common.cuh"
 
 namespace tsdx {
 namespace dev {

@@ -13,8 +13,8 @@
 
 namespace {
 using namespace tsdx;
-constexpr int kFeatWpc = 6;
-constexpr int kFeatSmem = kFeatWpc * 64 * dev::kFeatStride * (int)sizeof(double);
+constexpr int kFeatWpc = 8;
+constexpr int kFeatSmem = 0;
 constexpr int kTrainSmem = (int)sizeof(dev::TrainSmem);
 
 int finish(const char* what) {
@@ -36,7 +36,6 @@ API int tsdx_cuda_selector_features_f64(const double* A, int n, int64_t batch, c
   if (batch == 0) return TSDX_OK;
   if (!A || !features) return TSDX_ERR_NULL;
   auto kern = dev::features_kernel<kFeatWpc>;
-  if (int rc = host::prepare(kern, kFeatSmem)) return rc;
   const int grid = host::grid_for(kern, kFeatSmem, (batch + kFeatWpc - 1) / kFeatWpc, kFeatWpc * 32);
   kern<<<grid, kFeatWpc * 32, kFeatSmem, static_cast<cudaStream_t>(stream)>>>(A, n, batch, kind, kind_all, features);
   return finish("features kernel");

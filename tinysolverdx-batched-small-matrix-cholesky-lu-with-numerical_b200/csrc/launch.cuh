@@ -23,7 +23,7 @@ std::atomic<long long>& launch_counter();
 int device_sms(int dev);
 
 // Compiled padded sizes; a matrix of order n runs in the smallest NP >= n
-// (identity padding is exactly transparent to every result, see team.cuh).
+// (identity padding is exactly transparent to every result, see common.cuh).
 inline int np_of(int n) {
   return n <= 4 ? 4 : n <= 8 ? 8 : n <= 16 ? 16 : n <= 24 ? 24 : n <= 32 ? 32 : n <= 40 ? 40 : n <= 48 ? 48 : n <= 56 ? 56 : 64;
 }
@@ -134,7 +134,7 @@ int launch_trs(const SolveArgs<T>& a, int vec, cudaStream_t st) {
 
 // One fused pass: factor A (and solve B columns [b0, b0 + nrhs), nrhs <= 8).
 template <class T, bool CHOL>
-int run_team(const SolveArgs<T>& a, cudaStream_t st) {
+int run_blk(const SolveArgs<T>& a, cudaStream_t st) {
   const int np = np_of(a.n), rb = nrhs_bucket(a.nrhs);
   TSDX_NP_SWITCH(np, TSDX_RHS_SWITCH(rb, return (launch_blk<T, NP_, R_, CHOL>(a, st))));
   return 0;

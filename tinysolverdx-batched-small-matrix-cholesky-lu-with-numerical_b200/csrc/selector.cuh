@@ -6,7 +6,7 @@
 // whose refinement (ir.cuh) converges; the refinement's own residual check and
 // fp64 fallback make every prediction safe, a wrong one only costs time.
 //
-// Features (one warp per matrix, A staged once in shared memory as fp64). With
+// Features (one warp per matrix, one coalesced fp64 pass over A). With
 // d_i = |a_ii|, r_i = sum_j |a_ij| (row 1-norm), R_i = r_i - d_i, c_j = sum_i |a_ij|,
 // L(x) = log10(max(x, 1e-300)), every feature clipped to [-30, 30]:
 //   0 n/64             1 kind (0 SPD, 1 general)   2 L(max d) - L(min d)
@@ -39,7 +39,15 @@ constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kFeat * kHid, kOffW2 = kOffB1 + kHid
 constexpr int kTrainBlock = 64;   // samples per training block
 constexpr int kTrainThreads = 256;
 
-__device__ __forceinline__ double lg10(double x) { return log10(fmax(x, 1e-300)); }
+// log10(max(x, 1e-300)) to about 1e-7 absolute: the binary exponent exactly plus a
+// single-precision log2 of the mantissa (NaN maps to the clamp, like fmax does).
+__device__ __forceinline__ double lg10(double x) {
+  if (!(x >= 1e-300)) return -300.0;
+  if (x > 1.7976931348623157e308) return 309.0;
+  int e = 0;
+  const double m = frexp(x, &e);  // x = m 2^e, m in [0.5, 1)
+  return ((double)e + (double)__log2f((float)m)) * 0.30102999566398120;
+}
 __device__ __forceinline__ float clip30(double x) {
   if (!(x == x)) return 0.f;
   return (float)fmin(30.0, fmax(-30.0, x));
@@ -57,48 +65,78 @@ __device__ __forceinline__ double wmin(double v) {
   return v;
 }
 
-constexpr int kFeatStride = 65;  // doubles per staged row (n <= 64)
-
-// One warp per matrix; WPC warps per block, each with a 64 x 65 fp64 staging tile.
+// One warp per matrix, one coalesced pass over A in registers: lane c accumulates
+// columns c and c + 32, row 1-norms come from per-lane partial sums of 16-row
+// chunks folded by a transposing butterfly (lanes 2i and 2i + 1 end with row
+// 16 ch + i), then each row's norm is handed to the lane that owns it (row r:
+// lane r % 32, slot r / 32, the same lane that holds the diagonal a_rr as part
+// of column r).
 template <int WPC>
 __global__ void __launch_bounds__(WPC * 32) features_kernel(const double* __restrict__ A, int n, long long batch,
                                                             const signed char* kind, int kind_all, float* out) {
-  extern __shared__ __align__(16) double fsm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* S = fsm + warp * 64 * kFeatStride;
   const double INF = __longlong_as_double(0x7ff0000000000000LL);
   const long long nn = (long long)n * n;
   for (long long m = (long long)blockIdx.x * WPC + warp; m < batch; m += (long long)gridDim.x * WPC) {
     const double* Ag = A + m * nn;
-    for (int r = 0; r < n; ++r)
-      for (int c = lane; c < n; c += 32) S[r * kFeatStride + c] = __ldg(Ag + (long long)r * n + c);
-    __syncwarp();
-    double dmax = 0, dmin = INF, dsum = 0, rmax = 0, rmin = INF, amax = 0, fro = 0, lo = 0, up = 0;
+    double csum[2] = {0, 0}, cdg[2] = {0, 0}, cv[4] = {0, 0, 0, 0};
+    double amax = 0, lo = 0, up = 0;
+#pragma unroll
+    for (int ch = 0; ch < 4; ++ch) {
+      if (16 * ch < n) {
+        double pp[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int r = 16 * ch + j;
+          double acc = 0;
+          if (r < n) {
+            const double* row = Ag + (long long)r * n;
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+              const int c = lane + 32 * s;
+              if (c < n) {
+                const double v = __ldg(row + c), av = fabs(v), v2 = v * v;
+                acc += av;
+                csum[s] += av;
+                amax = fmax(amax, av);
+                if (c < r) lo += v2;
+                else if (c > r) up += v2;
+                else cdg[s] = av;
+              }
+            }
+          }
+          pp[j] = acc;
+        }
+#pragma unroll
+        for (int o = 16, w = 8; w >= 1; o >>= 1, w >>= 1) {
+          const bool hi = (lane & o) != 0;
+#pragma unroll
+          for (int j = 0; j < w; ++j) {
+            const double send = hi ? pp[j] : pp[j + w];
+            const double keep = hi ? pp[j + w] : pp[j];
+            pp[j] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+          }
+        }
+        cv[ch] = pp[0] + __shfl_xor_sync(0xffffffffu, pp[0], 1);
+      }
+    }
+    double dmax = 0, dmin = INF, dsum = 0, rmax = 0, rmin = INF, fro = lo + up;
     double dom = 0, gmin = INF, gsum = 0, gup = 0, sld = 0, sld2 = 0, slr = 0, slr2 = 0, rgmax = -INF, rgsum = 0;
     double offs = 0, cmax = 0, cmin = INF, slc = 0, slc2 = 0, cgmax = -INF, gnmin = INF;
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
-      const int r = lane + 32 * s;
+      const double a0 = __shfl_sync(0xffffffffu, cv[2 * s], 2 * (lane & 15));
+      const double a1 = __shfl_sync(0xffffffffu, cv[2 * s + 1], 2 * (lane & 15));
+      const int r = lane + 32 * s;  // row r and column r
       if (r < n) {
-        const double* row = S + r * kFeatStride;
-        double ra = 0, rowmax = 0, l2 = 0, u2 = 0;
-        for (int c = 0; c < n; ++c) {
-          const double v = row[c], av = fabs(v);
-          ra += av;
-          rowmax = fmax(rowmax, av);
-          if (c < r) l2 = fma(v, v, l2);
-          if (c > r) u2 = fma(v, v, u2);
-        }
-        const double d = fabs(row[r]), R = ra - d;
+        const double ra = (lane >> 4) ? a1 : a0;
+        const double d = cdg[s], R = ra - d;
+        fro += d * d;
         dmax = fmax(dmax, d);
         dmin = fmin(dmin, d);
         dsum += d;
         rmax = fmax(rmax, ra);
         rmin = fmin(rmin, ra);
-        amax = fmax(amax, rowmax);
-        lo += l2;
-        up += u2;
-        fro += l2 + u2 + d * d;
         dom += (d > R) ? 1.0 : 0.0;
         const double g = d - R;
         gmin = fmin(gmin, g);
@@ -113,17 +151,12 @@ __global__ void __launch_bounds__(WPC * 32) features_kernel(const double* __rest
         rgmax = fmax(rgmax, lr - ld);
         rgsum += lr - ld;
         offs += R;
-      }
-      const int c = lane + 32 * s;
-      if (c < n) {
-        double ca = 0;
-        for (int rr = 0; rr < n; ++rr) ca += fabs(S[rr * kFeatStride + c]);
+        const double ca = csum[s], lc = lg10(ca);
         cmax = fmax(cmax, ca);
         cmin = fmin(cmin, ca);
-        const double lc = lg10(ca);
         slc += lc;
         slc2 += lc * lc;
-        cgmax = fmax(cgmax, lc - lg10(fabs(S[c * kFeatStride + c])));
+        cgmax = fmax(cgmax, lc - ld);
       }
     }
     dmax = wmax(dmax); dmin = wmin(dmin); dsum = wsum(dsum); rmax = wmax(rmax); rmin = wmin(rmin);
@@ -135,7 +168,7 @@ __global__ void __launch_bounds__(WPC * 32) features_kernel(const double* __rest
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
       const int r = lane + 32 * s;
-      if (r < n && fabs(S[r * kFeatStride + r]) < 1e-8 * dmax) tiny += 1.0;
+      if (r < n && cdg[s] < 1e-8 * dmax) tiny += 1.0;
     }
     tiny = wsum(tiny);
     if (lane == 0) {

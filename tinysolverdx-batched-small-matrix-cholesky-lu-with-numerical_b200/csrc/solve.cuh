@@ -9,7 +9,7 @@
 // and multiplies by the reciprocal of the diagonal, so X agrees with the
 // reference to rounding.
 #pragma once
-#include "team.cuh"
+#include "common.cuh"
 
 namespace tsdx {
 namespace dev {

@@ -1,8 +1,12 @@
 """Learned per-matrix precision-tier selector for the mixed-precision solves.
 
 A small MLP (24 features -> 64 -> 64 -> 4 tiers) predicts, per matrix, the
-cheapest tier of {fp16, bf16, fp32, fp64} whose iterative refinement converges
-(status >= 0 within ``itmax`` corrections). Features, inference, the training
+lowest-precision tier of {fp16, bf16, fp32, fp64} whose iterative refinement
+converges (status >= 0 within ``itmax`` corrections). The solve policy then runs
+the tier, among the predicted one and those of higher precision, with the least
+measured cost per solve for the matrix's order and kind on this GPU (a cost table
+calibrated by selector_train.py and stored with the weights): where refinement
+does not pay, that is the plain fp64 solve. Features, inference, the training
 forward/backward pass and the Adam update are the library's own CUDA kernels
 (csrc/selector.cuh, C-ABI tsdx_cuda_selector_features_f64 / tsdx_cuda_mlp_* /
 tsdx_cuda_adam_step); labels come from running the refinement kernel itself on
@@ -46,7 +50,7 @@ def features(A, kind, stream=None):
 
 
 def label(A, b, spd, itmax=3, tol=1e-15, tiers=(0, 1, 2)):
-    """Label = the first tier in ``tiers`` (cheapest first) whose refinement converges
+    """Label = the first tier in ``tiers`` (lowest precision first) whose refinement converges
     within itmax corrections on (A, b); 3 (fp64) when none does. int8 CUDA tensor."""
     lab = torch.full((A.shape[0],), 3, dtype=torch.int8, device=A.device)
     for t in reversed(tiers):
@@ -77,6 +81,26 @@ class Selector:
         self.m = torch.zeros_like(self.params)
         self.v = torch.zeros_like(self.params)
         self.step = 0
+        self.cost = None    # (len(cost_n), 2 kinds, 4 tiers) ns per solve, or None
+        self.cost_n = None
+
+    # a predicted tier t means t converges; these tiers are expected to converge too
+    # (fp16 carries more precision than bf16 once the matrix is scaled into range)
+    CANDIDATES = {0: (0, 2, 3), 1: (1, 0, 2, 3), 2: (2, 3), 3: (3,)}
+
+    def policy_lut(self, n, spd):
+        """int8 (4,) map from predicted tier to the tier to run for order n and kind."""
+        lut = np.arange(4, dtype=np.int8)
+        if self.cost is not None:
+            i = int(np.argmin(np.abs(np.asarray(self.cost_n) - n)))
+            c = self.cost[i, 0 if spd else 1]
+            for t, cand in self.CANDIDATES.items():
+                lut[t] = min(cand, key=lambda u: c[u])
+        return lut
+
+    def policy(self, pred, n, spd):
+        lut = torch.from_numpy(self.policy_lut(n, spd)).to(pred.device)
+        return lut[pred.long()]
 
     # ---------------------------------------------------------------- inference
     def fit_normalizer(self, X):
@@ -145,11 +169,18 @@ class Selector:
 
     # --------------------------------------------------------------- persistence
     def state_dict(self):
-        return {"params": self.params.cpu().numpy(), "norm": self.norm.cpu().numpy()}
+        d = {"params": self.params.cpu().numpy(), "norm": self.norm.cpu().numpy()}
+        if self.cost is not None:
+            d["cost"] = np.asarray(self.cost)
+            d["cost_n"] = np.asarray(self.cost_n)
+        return d
 
     def load_state_dict(self, d):
         self.params = torch.as_tensor(np.asarray(d["params"], np.float32)).to(self.device).contiguous()
         self.norm = torch.as_tensor(np.asarray(d["norm"], np.float32)).to(self.device).contiguous()
+        if "cost" in d:
+            self.cost = np.asarray(d["cost"], np.float64)
+            self.cost_n = np.asarray(d["cost_n"], np.int64)
 
     def save(self, path):
         np.savez(path, **self.state_dict())
@@ -163,10 +194,18 @@ class Selector:
 
     # -------------------------------------------------------------------- solve
     def solve(self, A, b, spd, itmax=3, tol=1e-15):
-        """Predict a tier per matrix, then refine on it (fp64 fallback on a miss).
+        """Predict the lowest converging tier per matrix, run the cheapest tier at or
+        above it (policy_lut), refine, fall back to fp64 on a miss.
         A (batch, n, n) float64, b (batch, n) float64 overwritten by x.
-        Returns (info, status, bwd, tier)."""
+        Returns (info, status, bwd, tier run)."""
+        n = A.shape[-1]
+        lut = self.policy_lut(n, spd)
+        if (lut == 3).all():
+            # no tier is cheaper than fp64 at this order on this GPU: skip the features
+            # and the network, solve in plain fp64
+            info, status, bwd = device.ir(A, b, spd, default_tier=3, itmax=itmax, tol=tol)
+            return info, status, bwd, torch.full_like(status, 3, dtype=torch.int8)
         X = features(A, 0 if spd else 1)
-        tier = self.predict(X)
+        tier = torch.from_numpy(lut).to(A.device)[self.predict(X).long()].contiguous()
         info, status, bwd = device.ir(A, b, spd, tier=tier, itmax=itmax, tol=tol)
         return info, status, bwd, tier
