@@ -90,11 +90,11 @@ def peaks():
 
 def traffic_from_profiles(name):
     """dram bytes per launch recorded from an ncu capture in profiles/ (or None)."""
-    p = ROOT / "profiles" / f"{name}_ncu.md"
-    if not p.exists():
-        return None
-    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
-    return float(m.group(1)) if m else None
+    for p in sorted((ROOT / "profiles").glob(f"*__{name}.md")):
+        m = re.search(r"traffic_bytes_per_launch[^:]*:\s*([0-9.eE+]+)", p.read_text())
+        if m:
+            return float(m.group(1))
+    return None
 
 
 # ---------------------------------------------------------------- clocks (NVML)
