@@ -119,6 +119,30 @@ int tsdx_cuda_posv_ir_f64(const double* A, int n, int64_t batch, double* B, cons
                           int default_tier, int itmax, double tol, int* info, int* status, double* bwd,
                           void* stream);
 
+/* ---- emulated fp16 / bf16 on the GPU (host pointers, synchronous) -----------------
+ * The reference's per-operation-rounding formats (precision.hpp:41-97), which it runs
+ * only on the CPU (batched.hpp:130-132), bit-identical to its CPU results. Storage is
+ * float64 as in the runtime API (runtime.cpp:95-141); fmt 0 = fp16, 1 = bf16.
+ *   factor: lu = 0 Cholesky (A <- L, info), lu = 1 LU (A <- L\U, piv, info)
+ *   solve:  lu = 0 B <- (L L^T)^{-1} B, lu = 1 B <- (P L U)^{-1} B */
+int tsdx_cuda_emu_factor_host(int fmt, int lu, double* A, int n, int64_t batch, int* piv, int* info);
+int tsdx_cuda_emu_solve_host(int fmt, int lu, const double* F, const int* piv, int n, int64_t batch, double* B,
+                             int nrhs);
+
+/* ---- error metrics on the GPU ------------------------------------------------------
+ * The reference's ground-truth metrics (src/runtime.cpp:194-242, long double on the
+ * CPU) computed per matrix in double-double arithmetic on the device; float64
+ * inputs, device pointers, out (batch) float64.
+ *   solve_backward_error  ||b - A x||_2 / (||A||_F ||x||_2 + ||b||_2)   runtime.cpp:230-242
+ *   lu_backward_error     ||P A - L U||_F / ||A||_F  (packed LU, pivots)  runtime.cpp:208-228
+ *   chol_backward_error   ||A - L L^T||_F / ||A||_F                      runtime.cpp:194-206 */
+int tsdx_cuda_solve_backward_error_f64(const double* A, const double* x, const double* b, int n, int64_t batch,
+                                       double* out, void* stream);
+int tsdx_cuda_lu_backward_error_f64(const double* A, const double* LU, const int* piv, int n, int64_t batch,
+                                    double* out, void* stream);
+int tsdx_cuda_chol_backward_error_f64(const double* A, const double* L, int n, int64_t batch, double* out,
+                                      void* stream);
+
 /* ---- learned precision-tier selector (no reference counterpart) -------------------
  * A 24 -> 64 -> 64 -> 4 MLP over cheap per-matrix features predicts the cheapest
  * tier (0 fp16, 1 bf16, 2 fp32, 3 fp64) whose refinement converges; the tier array

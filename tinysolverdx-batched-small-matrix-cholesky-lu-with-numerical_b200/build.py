@@ -28,7 +28,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden",
                   "-I" + str(CSRC), "-I" + str(ROOT / "include")]
-CUDA_SOURCES = ["capi.cu", "k_lu_f32.cu", "k_lu_f64.cu", "k_chol_f32.cu", "k_chol_f64.cu", "k_ir.cu", "k_stream_f32.cu", "k_stream_f64.cu", "k_stream_noalloc.cu", "k_selector.cu"]
+CUDA_SOURCES = ["capi.cu", "k_lu_f32.cu", "k_lu_f64.cu", "k_chol_f32.cu", "k_chol_f64.cu", "k_ir.cu", "k_stream_f32.cu", "k_stream_f64.cu", "k_stream_noalloc.cu", "k_selector.cu", "k_metrics.cu", "k_emu.cu"]
 
 
 def _deps(path, seen=None):

@@ -13,7 +13,9 @@
 // product and subtraction for n >= 17; the scalar dot product in 16-byte groups).
 // Nothing here falls back silently: Backend::Cuda without a device throws
 // std::runtime_error, exactly like the reference built without CUDA
-// (batched.hpp:132).
+// (batched.hpp:132). The emulated fp16/bf16 formats, which the reference refuses
+// on Backend::Cuda (batched.hpp:130-132), run on the GPU here, bit-identical to
+// the CPU path (tsdx_cuda_emu_*_host).
 #pragma once
 
 #include <atomic>
@@ -382,13 +384,33 @@ template <class T, class S> void from_t(const std::vector<T>& v, S* x) {
 }
 }  // namespace detail
 
+namespace detail {
+// Emulated formats on the GPU (tsdx_cuda_emu_*_host, bit-identical to the CPU path):
+// the reference throws here (batched.hpp:130-132); this build runs them instead.
+template <class T> constexpr int emu_fmt() { return std::is_same<T, Half>::value ? 0 : 1; }
+template <class S> std::vector<double> f64_copy(const S* x, std::int64_t count) {
+  return std::vector<double>(x, x + count);
+}
+template <class S> void f64_back(const std::vector<double>& v, S* x) {
+  for (std::size_t i = 0; i < v.size(); ++i) x[i] = static_cast<S>(v[i]);
+}
+}  // namespace detail
+
 template <class S>
 void cholesky(Precision p, S* A, int n, std::int64_t batch, int* info, Backend be = Backend::Auto) {
   detail::with_precision(p, [&](auto tag) {
     using T = decltype(tag);
     if constexpr (std::is_same<T, S>::value) cholesky_batched<T>(A, n, batch, info, be);
     else {
-      if (be == Backend::Cuda && !is_native<T>::value) throw std::runtime_error("CUDA backend unavailable for this build/precision");
+      if constexpr (!is_native<T>::value) {
+        if (be == Backend::Cuda) {
+          detail::check_dims(n, batch);
+          auto w = detail::f64_copy(A, batch * n * n);
+          detail::check_cuda(tsdx_cuda_emu_factor_host(detail::emu_fmt<T>(), 0, w.data(), n, batch, nullptr, info));
+          detail::f64_back(w, A);
+          return;
+        }
+      }
       auto v = detail::to_t<T>(A, batch * n * n);
       cholesky_batched<T>(v.data(), n, batch, info, be);
       detail::from_t(v, A);
@@ -401,7 +423,16 @@ void lu(Precision p, S* A, int n, std::int64_t batch, int* piv, int* info, Backe
     using T = decltype(tag);
     if constexpr (std::is_same<T, S>::value) lu_batched<T>(A, n, batch, piv, info, be);
     else {
-      if (be == Backend::Cuda && !is_native<T>::value) throw std::runtime_error("CUDA backend unavailable for this build/precision");
+      if constexpr (!is_native<T>::value) {
+        if (be == Backend::Cuda) {
+          detail::check_dims(n, batch);
+          if (!piv) throw std::invalid_argument("piv must not be null");
+          auto w = detail::f64_copy(A, batch * n * n);
+          detail::check_cuda(tsdx_cuda_emu_factor_host(detail::emu_fmt<T>(), 1, w.data(), n, batch, piv, info));
+          detail::f64_back(w, A);
+          return;
+        }
+      }
       auto v = detail::to_t<T>(A, batch * n * n);
       lu_batched<T>(v.data(), n, batch, piv, info, be);
       detail::from_t(v, A);
@@ -412,7 +443,16 @@ template <class S>
 void cholesky_solve(Precision p, const S* L, int n, std::int64_t batch, S* B, int nrhs, Backend be = Backend::Auto) {
   detail::with_precision(p, [&](auto tag) {
     using T = decltype(tag);
-    if (be == Backend::Cuda && !is_native<T>::value) throw std::runtime_error("CUDA backend unavailable for this build/precision");
+    if constexpr (!is_native<T>::value) {
+      if (be == Backend::Cuda) {
+        detail::check_dims(n, batch);
+        auto l = detail::f64_copy(L, batch * n * n);
+        auto b = detail::f64_copy(B, batch * n * nrhs);
+        detail::check_cuda(tsdx_cuda_emu_solve_host(detail::emu_fmt<T>(), 0, l.data(), nullptr, n, batch, b.data(), nrhs));
+        detail::f64_back(b, B);
+        return;
+      }
+    }
     auto l = detail::to_t<T>(L, batch * n * n);
     auto b = detail::to_t<T>(B, batch * n * nrhs);
     cholesky_solve_batched<T>(l.data(), n, batch, b.data(), nrhs, be);
@@ -423,7 +463,16 @@ template <class S>
 void lu_solve(Precision p, const S* LU, const int* piv, int n, std::int64_t batch, S* B, int nrhs, Backend be = Backend::Auto) {
   detail::with_precision(p, [&](auto tag) {
     using T = decltype(tag);
-    if (be == Backend::Cuda && !is_native<T>::value) throw std::runtime_error("CUDA backend unavailable for this build/precision");
+    if constexpr (!is_native<T>::value) {
+      if (be == Backend::Cuda) {
+        detail::check_dims(n, batch);
+        auto l = detail::f64_copy(LU, batch * n * n);
+        auto b = detail::f64_copy(B, batch * n * nrhs);
+        detail::check_cuda(tsdx_cuda_emu_solve_host(detail::emu_fmt<T>(), 1, l.data(), piv, n, batch, b.data(), nrhs));
+        detail::f64_back(b, B);
+        return;
+      }
+    }
     auto l = detail::to_t<T>(LU, batch * n * n);
     auto b = detail::to_t<T>(B, batch * n * nrhs);
     lu_solve_batched<T>(l.data(), piv, n, batch, b.data(), nrhs, be);

@@ -80,3 +80,39 @@ def ir(A, x, spd, tier=None, default_tier=2, itmax=3, tol=1e-15, stream=None):
     capi.check(capi.call(name, capi.ptr(A), n, batch, capi.ptr(x), capi.ptr(tier), int(default_tier), int(itmax),
                          float(tol), capi.ptr(info), capi.ptr(status), capi.ptr(bwd), capi.stream_ptr(stream)), name)
     return info, status, bwd
+
+
+def _metric_out(A):
+    return torch.empty(A.shape[0], dtype=torch.float64, device=A.device)
+
+
+def solve_backward_error(A, x, b, stream=None):
+    """||b - A x|| / (||A||_F ||x|| + ||b||) per matrix, double-double on the device
+    (the reference's runtime.cpp:230-242 metric). A (batch, n, n), x and b (batch, n), float64."""
+    for t, nm in ((A, "A"), (x, "x"), (b, "b")):
+        _check(t, nm, torch.float64)
+    out = _metric_out(A)
+    capi.check(capi.call("tsdx_cuda_solve_backward_error_f64", capi.ptr(A), capi.ptr(x), capi.ptr(b), A.shape[-1],
+                         A.shape[0], capi.ptr(out), capi.stream_ptr(stream)), "solve_backward_error")
+    return out
+
+
+def lu_backward_error(A, LU, piv, stream=None):
+    """||P A - L U||_F / ||A||_F per matrix (runtime.cpp:208-228), double-double on the device."""
+    _check(A, "A", torch.float64)
+    _check(LU, "LU", torch.float64)
+    _check(piv, "piv", torch.int32)
+    out = _metric_out(A)
+    capi.check(capi.call("tsdx_cuda_lu_backward_error_f64", capi.ptr(A), capi.ptr(LU), capi.ptr(piv), A.shape[-1],
+                         A.shape[0], capi.ptr(out), capi.stream_ptr(stream)), "lu_backward_error")
+    return out
+
+
+def chol_backward_error(A, L, stream=None):
+    """||A - L L^T||_F / ||A||_F per matrix (runtime.cpp:194-206), double-double on the device."""
+    _check(A, "A", torch.float64)
+    _check(L, "L", torch.float64)
+    out = _metric_out(A)
+    capi.check(capi.call("tsdx_cuda_chol_backward_error_f64", capi.ptr(A), capi.ptr(L), A.shape[-1], A.shape[0],
+                         capi.ptr(out), capi.stream_ptr(stream)), "chol_backward_error")
+    return out
