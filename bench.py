@@ -57,6 +57,8 @@ SPECIAL = {
                   "kappa log-uniform [1e1,1e8], RHS count uniform {1,2,4,8}, one graph-captured launch sequence",
     "selector": "learned tier selector evaluation: 1,048,576 matrices, n uniform {8..64}, half SPD / half LU, "
                 "kappa log-uniform [1e0,1e14], 1 RHS, selector tiers + fp64 refinement + fp64 fallback",
+    "ir_fp32_n64": "fixed tier: fp32 factorization + fp64 refinement (tolerance 1e-15, at most 3 corrections, fp64 "
+                   "fallback), n=64 general LU, batch 65,536, 1 RHS, kappa log-uniform [1e1,1e3]",
 }
 
 
@@ -589,8 +591,9 @@ def _ir_workload(a, world, rank, local, device, dist):
     extra["bwd_max_ratio_vs_plain_fp64"] = round(errs["selector"]["max"] / errs["plain_fp64"]["max"], 3)
     extra["speedup_vs_plain_fp64"] = round(value / world / extra["plain_fp64"]["solves_per_s"], 3)
     bytes_step = batch * (8 * (n * n + 2 * n) + 4)
-    roof = _roof(bytes_step, ms, "ir_kernel<64> (+ features, mlp_forward, fp64 fallback blk_kernel)",
-                 traffic=traffic_from_profiles("ir_n64"))
+    routed = "every matrix routed to fp64 by the calibrated policy: blk2_kernel x-only" if tiers.get("fp64") == batch \
+        else "ir_kernel<64> + features + mlp_forward + fp64 fallback"
+    roof = _roof(bytes_step, ms, routed, traffic=traffic_from_profiles("ir_n64"))
     # end to end: pinned host A and b in, x and info out, every step
     e2e = None
     if not a.skip_e2e:
@@ -794,9 +797,47 @@ def _selector_workload(a, world, rank, local, device, dist):
     return value, ms, "f64 (tiers fp16/bf16/fp32 factor, fp64 residual)", cfg, roof, None, None, clk, launches, extra
 
 
+def _ir_fixed_workload(a, world, rank, local, device, dist):
+    import torch
+    M, dev = _pkg("matrices"), _pkg("device")
+    n, batch = 64, a.batch or 65536
+    A = M.torch_stack("general", n, batch, 1e1, 1e3, 5150 + rank, device=device).contiguous()
+    g = torch.Generator(device=device)
+    g.manual_seed(5151 + rank)
+    b = torch.randn(batch, n, generator=g, device=device, dtype=torch.float64)
+    pool = max(2, min(a.steps + a.warmup, 24))
+    xs = [b.clone() for _ in range(pool)]
+    ms, clk, launches = _timed(lambda i: dev.ir(A, xs[i % pool], False, default_tier=2), a, world, local, device, dist)
+    value = world * batch / (ms * 1e-3)
+    x = b.clone()
+    _, status, _ = dev.ir(A, x, False, default_tier=2)
+    xp = b.clone()
+    tp = _once(lambda: dev.ir(A, xp, False, default_tier=3))
+    extra = {"refined_without_fallback": float((status >= 0).float().mean().item()),
+             "corrections_median": float(status[status >= 0].float().median().item()),
+             "plain_fp64": {"solves_per_s": round(batch / (tp * 1e-3), 1), "ms": round(tp, 4)},
+             "speedup_vs_plain_fp64": round(value / world / (batch / (tp * 1e-3)), 3),
+             "backward_error": {"ir_fp32": _stats(dev.solve_backward_error(A, x, b)),
+                                "plain_fp64": _stats(dev.solve_backward_error(A, xp, b))}}
+    roof = _roof(batch * (8 * (n * n + 2 * n) + 4), ms, "ir_kernel<64,LU> (fp32 tier)",
+                 traffic=traffic_from_profiles("ir_fp32_n64"))
+    cpu = None
+    if rank == 0 and world == 1 and not a.skip_cpu:
+        rng = np.random.default_rng(6)
+        v, thr, kl = _cpu_solves([("gesv", M.general(rng, 4096, n, M.log_uniform(rng, 4096, 1e1, 1e3)),
+                                   rng.standard_normal((4096, n, 1)))])
+        cpu = {"value": round(v, 1), "unit": "solves/s", "cores": thr, "kind": kl,
+               "sample": "4096 n=64 fp64 gesv, 1 RHS (the reference has no mixed-precision path)"}
+    cfg = {"workload": SPECIAL["ir_fp32_n64"], "global_batch": world * batch, "batch_per_gpu": batch,
+           "parallelism": f"batch sharded over {world} GPU(s), no collective",
+           "l2": "inputs larger than L2 (2.1 GB of A per step)"}
+    return value, ms, "f64 (fp32 factor, fp64 residual)", cfg, roof, cpu, None, clk, launches, extra
+
+
 def run_ours_special(a):
     world, rank, local, device, dist = _dist_setup()
-    fn = {"ir_n64": _ir_workload, "stream_f32": _stream_workload, "selector": _selector_workload}[a.workload]
+    fn = {"ir_n64": _ir_workload, "stream_f32": _stream_workload, "selector": _selector_workload,
+          "ir_fp32_n64": _ir_fixed_workload}[a.workload]
     value, ms, dt, cfg, roof, cpu, e2e, clk, launches, extra = fn(a, world, rank, local, device, dist)
     if rank == 0:
         _emit(a, world, value, ms, dt, cfg, roof, cpu, e2e, clk, launches, extra)
@@ -827,8 +868,8 @@ def run_reference_special(a):
                                    rng.standard_normal((16, ni, r)).astype(np.float32)))
         sample = "16 fp32 matrices per (kind, n, nrhs) for every n in 2..64, both kinds, nrhs in {1,2,4,8} (8064)"
     else:
-        sizes = (64,) if a.workload == "ir_n64" else (8, 24, 40, 56, 64)
-        khi = 1e12 if a.workload == "ir_n64" else 1e14
+        sizes = (64,) if a.workload in ("ir_n64", "ir_fp32_n64") else (8, 24, 40, 56, 64)
+        khi = {"ir_n64": 1e12, "ir_fp32_n64": 1e3}.get(a.workload, 1e14)
         groups = []
         for ni in sizes:
             for kk in ("posv", "gesv"):
@@ -843,7 +884,7 @@ def run_reference_special(a):
             vals.append(v)
     value = float(np.median(vals))
     cfg = {"workload": SPECIAL[a.workload]}
-    per_step = {"ir_n64": 131072, "stream_f32": 1048576, "selector": 1048576}[a.workload]
+    per_step = {"ir_n64": 131072, "stream_f32": 1048576, "selector": 1048576, "ir_fp32_n64": 65536}[a.workload]
     cfg["global_batch"] = per_step
     _emit(a, world, value, per_step / value * 1e3, "f32" if a.workload == "stream_f32" else "f64", cfg, None,
           {"value": round(value, 1), "unit": "solves/s", "cores": thr, "kind": kl, "sample": sample},
