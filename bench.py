@@ -320,7 +320,9 @@ def run_ours(a):
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": src,
             "algorithmic_bytes_per_launch": per_launch,
-            "kernel": (f"blk2_kernel<{dt},NP={n},LU> (two warps per matrix)" if kind == "gesv" and dt == "f64"
+            "kernel": (f"blk3_kernel<{dt},NP={n},LU> (two warps per matrix, look-ahead)" if kind == "gesv"
+                       and dt == "f64" and n > 56 else
+                       f"blk2_kernel<{dt},NP={n},LU> (two warps per matrix)" if kind == "gesv" and dt == "f64"
                        and n > 40 else f"blk_kernel<{dt},NP={n},{'LU' if kind == 'gesv' else 'Cholesky'}>"),
             "gflops": round(batch * flops(kind, n, nrhs) / (ms_step * 1e-3) / 1e9, 1)}
 

@@ -9,7 +9,7 @@
 
 #include "blk.cuh"
 #include "solve.cuh"
-#include "blk2.cuh"
+#include "blk3.cuh"
 
 namespace tsdx {
 namespace host {
@@ -81,7 +81,7 @@ constexpr int blk_lanes() {
   return blk_wpc<T, NP, NRHS, 16>() == 16 ? 16 : 0;
 }
 
-// Two warps per matrix (blk2.cuh) for float64 LU of padded order 48..64: measured on
+// Two warps per matrix (blk2.cuh) for float64 LU of padded order 48..56: measured on
 // B200 against one warp per matrix at 65,536-131,072 matrices with 4 right-hand
 // sides, 1.10x (order 48), 1.22x (56), 1.10x (64); slower at 40 and in float32.
 template <class T, int NP, int NRHS>
@@ -101,8 +101,29 @@ int launch_blk2(const SolveArgs<T>& a, cudaStream_t st) {
   return 0;
 }
 
+// Two warps per matrix with look-ahead (blk3.cuh) for float64 LU of padded order 64:
+// 1.10x the two-warp kernel (1.18x at n = 61) on B200, 65,536 matrices, 4 right-hand
+// sides; slower than it at orders 40..56.
+template <class T, int NP, int NRHS>
+int launch_blk3(const SolveArgs<T>& a, cudaStream_t st) {
+  using C = dev::Blk3Cfg<T, NP, NRHS>;
+  constexpr int FIT = (227 * 1024) / C::TEAMB;
+  constexpr int TPC = FIT < 1 ? 1 : (FIT > 8 ? 8 : FIT);
+  constexpr int SMEM = TPC * C::TEAMB;
+  auto kern = dev::blk3_kernel<T, NP, NRHS, TPC>;
+  if (int rc = prepare(kern, SMEM)) return rc;
+  const long long ctas = (a.batch + TPC - 1) / TPC;
+  const int grid = grid_for(kern, SMEM, ctas, TPC * 64);
+  kern<<<grid, TPC * 64, SMEM, st>>>(a);
+  launch_counter().fetch_add(1);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) { set_cuda_error(e, "kernel launch"); return -5; }
+  return 0;
+}
+
 template <class T, int NP, int NRHS, bool CHOL>
 int launch_blk(const SolveArgs<T>& a, cudaStream_t st) {
+  if constexpr (!CHOL && sizeof(T) == 8 && NP == 64) return launch_blk3<T, NP, NRHS>(a, st);
   if constexpr (!CHOL && sizeof(T) == 8 && NP >= 48) return launch_blk2<T, NP, NRHS>(a, st);
   constexpr int GO = blk_lanes<T, NP, NRHS, CHOL>();
   using C = dev::BlkCfg<T, NP, NRHS, GO>;
