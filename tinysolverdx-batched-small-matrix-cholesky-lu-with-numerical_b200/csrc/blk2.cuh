@@ -240,8 +240,9 @@ __global__ void __launch_bounds__(TPC * 64, 1) blk2_kernel(SolveArgs<T> p) {
     const long long m = base + team;
     MatJob<T> j;
     j.live = m < p.batch && !(p.status && p.status[m] >= 0);
-    // a team with nothing to do skips the round (its barrier id is private to it)
-    if (!j.live && m >= p.batch) continue;
+    // a team with nothing to do (past the batch, or a matrix the status mask marks
+    // as already solved) skips the round; its barrier id is private to it
+    if (!j.live) continue;
     const long long mm = j.live ? m : 0;
     j.A = p.A + mm * nn;
     j.Aout = p.wf ? p.A + mm * nn : nullptr;

@@ -349,6 +349,7 @@ __global__ void __launch_bounds__(TPC * 64, 1) blk3_kernel(SolveArgs<T> p) {
     if (m >= p.batch) continue;  // team-uniform; barrier ids are private to the team
     MatJob<T> j;
     j.live = !(p.status && p.status[m] >= 0);
+    if (!j.live) continue;  // already solved (status mask): nothing to read or write
     const long long mm = m;
     j.A = p.A + mm * nn;
     j.Aout = p.wf ? p.A + mm * nn : nullptr;
