@@ -32,7 +32,10 @@ struct Blk3Cfg {
   static_assert(NP > 32 && NP <= 64 && PB == CH, "two row slots per lane, panel width = chunk width");
 };
 
-template <class T, int NP, int NRHS>
+// SC: the pivot steps of a panel counted in chunk updates. When the update warp has
+// R chunks left and R - 1 - SC >= 2, the panel warp takes the last (R - 1 - SC) / 2
+// of them, so both warps reach the panel barrier at about the same time.
+template <class T, int NP, int NRHS, int SC = 99>
 __device__ __forceinline__ void lu3_matrix(unsigned char* M, const MatJob<T>& j, int t, int bar) {
   using C = Blk3Cfg<T, NP, NRHS>;
   using K = typename KeyT<T>::U;
@@ -47,6 +50,50 @@ __device__ __forceinline__ void lu3_matrix(unsigned char* M, const MatJob<T>& j,
   unsigned* zpub = reinterpret_cast<unsigned*>(amask + 1);
   auto at = [&](int r, int c) -> T& { return *reinterpret_cast<T*>(M + r * RS + c * TS); };
   auto vat = [&](int r, int c) -> VT& { return *reinterpret_cast<VT*>(M + r * RS + c * TS); };
+  // panel k0's update on chunks [jb, je) of the lane's rows (lv: their panel values,
+  // ra: still active), the chain of blk.cuh's trailing update
+  auto update_chunks = [&](const T (&lv)[MR][PB], const bool (&ra)[MR], const int (&ordp)[PB], unsigned zb,
+                           int jb, int je) {
+    for (int jc = jb; jc < je; jc += CH) {
+      T acc[MR][CH];
+#pragma unroll
+      for (int s = 0; s < MR; ++s) {
+        const int rr = ra[s] ? lane + 32 * s : 0;
+#pragma unroll
+        for (int c0 = 0; c0 < CH; c0 += VN) {
+          const VT v = vat(rr, jc + c0);
+#pragma unroll
+          for (int q = 0; q < VN; ++q) acc[s][c0 + q] = V::get(v, q);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < PB; ++i) {
+        if ((zb >> i) & 1u) continue;
+#pragma unroll
+        for (int c0 = 0; c0 < CH; c0 += VN) {
+          const VT v = vat(ordp[i], jc + c0);
+#pragma unroll
+          for (int q = 0; q < VN; ++q) {
+            const T u = V::get(v, q);
+#pragma unroll
+            for (int s = 0; s < MR; ++s) acc[s][c0 + q] = fma_(-lv[s][i], u, acc[s][c0 + q]);
+          }
+        }
+      }
+#pragma unroll
+      for (int s = 0; s < MR; ++s) {
+        if (!ra[s]) continue;
+        const int r = lane + 32 * s;
+#pragma unroll
+        for (int c0 = 0; c0 < CH; c0 += VN) {
+          VT w;
+#pragma unroll
+          for (int q = 0; q < VN; ++q) V::set(w, q, acc[s][c0 + q]);
+          vat(r, jc + c0) = w;
+        }
+      }
+    }
+  };
 
   // ---- stage A (rows dealt to the two warps) and the right-hand sides
   if (j.live) {
@@ -210,6 +257,11 @@ __device__ __forceinline__ void lu3_matrix(unsigned char* M, const MatJob<T>& j,
     }
     team_sync(bar);  // T: U12 in place
     if (j1 >= NC) continue;
+    // chunks beyond the next one: the update warp takes [j1 + CH, jsplit), the
+    // panel warp the rest
+    const int rem = NC > j1 + CH ? (NC - j1 - CH + CH - 1) / CH : 0;
+    const int xtra = rem - 1 - SC >= 2 ? (rem - 1 - SC) / 2 : 0;
+    const int jsplit = j1 + CH + (rem - xtra) * CH;
     if (warp == 0) {
       // ---- 3a. the next chunk (panel p + 1, or the right-hand sides after the last
       // panel) for the panel warp's rows, kept in registers for the next pivot steps
@@ -238,6 +290,12 @@ __device__ __forceinline__ void lu3_matrix(unsigned char* M, const MatJob<T>& j,
               nxt[s][c0 + q] = act[s] ? fma_(-pan[s][i], u, nxt[s][c0 + q]) : nxt[s][c0 + q];
           }
         }
+      }
+      if (xtra > 0) {
+        bool ra[MR];
+#pragma unroll
+        for (int s = 0; s < MR; ++s) ra[s] = act[s] && lane + 32 * s < NP;
+        update_chunks(pan, ra, ordp, zb, jsplit, NC);
       }
       if (p + 1 == NPAN) {
         // the right-hand-side chunk: write it back (the active rows' values changed)
@@ -276,45 +334,7 @@ __device__ __forceinline__ void lu3_matrix(unsigned char* M, const MatJob<T>& j,
           for (int q = 0; q < VN; ++q) lr[s][i0 + q] = V::get(v, q);
         }
       }
-      for (int jc = j1 + CH; jc < NC; jc += CH) {
-        T acc[MR][CH];
-#pragma unroll
-        for (int s = 0; s < MR; ++s) {
-          const int rr = ra[s] ? lane + 32 * s : 0;
-#pragma unroll
-          for (int c0 = 0; c0 < CH; c0 += VN) {
-            const VT v = vat(rr, jc + c0);
-#pragma unroll
-            for (int q = 0; q < VN; ++q) acc[s][c0 + q] = V::get(v, q);
-          }
-        }
-#pragma unroll
-        for (int i = 0; i < PB; ++i) {
-          if ((zb >> i) & 1u) continue;
-#pragma unroll
-          for (int c0 = 0; c0 < CH; c0 += VN) {
-            const VT v = vat(ordp[i], jc + c0);
-#pragma unroll
-            for (int q = 0; q < VN; ++q) {
-              const T u = V::get(v, q);
-#pragma unroll
-              for (int s = 0; s < MR; ++s) acc[s][c0 + q] = fma_(-lr[s][i], u, acc[s][c0 + q]);
-            }
-          }
-        }
-#pragma unroll
-        for (int s = 0; s < MR; ++s) {
-          if (!ra[s]) continue;
-          const int r = lane + 32 * s;
-#pragma unroll
-          for (int c0 = 0; c0 < CH; c0 += VN) {
-            VT w;
-#pragma unroll
-            for (int q = 0; q < VN; ++q) V::set(w, q, acc[s][c0 + q]);
-            vat(r, jc + c0) = w;
-          }
-        }
-      }
+      update_chunks(lr, ra, ordp, zb, j1 + CH, jsplit);
     }
     // the next S barrier orders the update warp's writes before the next U12
   }
@@ -337,7 +357,7 @@ __device__ __forceinline__ void lu3_matrix(unsigned char* M, const MatJob<T>& j,
   team_sync(bar);
 }
 
-template <class T, int NP, int NRHS, int TPC>
+template <class T, int NP, int NRHS, int TPC, int SC = 99>
 __global__ void __launch_bounds__(TPC * 64, 1) blk3_kernel(SolveArgs<T> p) {
   using C = Blk3Cfg<T, NP, NRHS>;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -360,7 +380,7 @@ __global__ void __launch_bounds__(TPC * 64, 1) blk3_kernel(SolveArgs<T> p) {
     j.ldb = p.ldb;
     j.b0 = p.b0;
     j.nrhs = p.nrhs;
-    lu3_matrix<T, NP, NRHS>(M, j, t, 1 + team);
+    lu3_matrix<T, NP, NRHS, SC>(M, j, t, 1 + team);
   }
 }
 
