@@ -13,8 +13,8 @@
 // Schedule. A counting sort (histogram, scan, scatter) orders the matrices by
 // bucket = (kind, padded order NP in {8, 16, ..., 64}, right-hand-side class
 // {<= 2, <= 8}); each bucket is cut into work units of S matrices (S = 32/G
-// segments per warp for NP <= 32, or one warp per matrix when the tuned schedule
-// asks for it). One persistent launch then drains the units through a global
+// segments per warp for NP <= 32: 4 up to order 16, 2 up to 32; or one warp per
+// matrix when the tuned schedule asks for it). One persistent launch then drains the units through a global
 // atomic queue, largest order first, so at any moment the SMs run mostly the same
 // code variant and the smallest units fill the tail; each unit is the same
 // per-matrix body (blk.cuh) as the dense kernels, so the results are
@@ -57,12 +57,12 @@ __device__ __forceinline__ int bucket_of(int kind, int n, int nrhs) {
   return ((kStreamClasses - 1 - np_class(n)) * 2 + (kind ? 1 : 0)) * 2 + (nrhs > 2 ? 1 : 0);
 }
 __device__ __forceinline__ int bucket_class(int b) { return kStreamClasses - 1 - (b >> 2); }
-// matrices per work unit for a bucket: 4 (n <= 8) or 2 (9 <= n <= 32) segments
+// matrices per work unit for a bucket: 4 (n <= 16) or 2 (17 <= n <= 32) segments
 // share a warp unless sched bit c (order class c = 0..3) asks for one matrix per warp
 __device__ __forceinline__ int unit_size(int b, unsigned sched) {
   const int c = bucket_class(b);
   if (c >= 4 || ((sched >> c) & 1u)) return 1;
-  return c == 0 ? 4 : 2;
+  return c <= 1 ? 4 : 2;
 }
 
 // Histogram: block-local counts in shared memory, one global atomic per bucket per block.
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(WPC * 32, 1) stream_kernel(StreamArgs<T> a) {
   else { TSDX_SU_KIND(NP_, 2, G_); }
     switch (c) {
       case 0: if (one) { TSDX_SU_RHS(8, 32) } else { TSDX_SU_RHS(8, 8) } break;
-      case 1: if (one) { TSDX_SU_RHS(16, 32) } else { TSDX_SU_RHS(16, 16) } break;
+      case 1: if (one) { TSDX_SU_RHS(16, 32) } else { TSDX_SU_RHS(16, 8) } break;
       case 2: if (one) { TSDX_SU_RHS(24, 32) } else { TSDX_SU_RHS(24, 16) } break;
       case 3: if (one) { TSDX_SU_RHS(32, 32) } else { TSDX_SU_RHS(32, 16) } break;
       case 4: TSDX_SU_RHS(40, 32) break;

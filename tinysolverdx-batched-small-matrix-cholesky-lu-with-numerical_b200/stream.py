@@ -20,7 +20,7 @@ from . import capi
 
 CHOLESKY, LU = 0, 1
 # sched bit c (order class c: n in 1..8, 9..16, 17..24, 25..32) set -> those matrices
-# run one per warp; clear -> four (class 0) or two (classes 1-3) share a warp
+# run one per warp; clear -> four (classes 0-1) or two (classes 2-3) share a warp
 SCHED_BITS = 4
 
 
