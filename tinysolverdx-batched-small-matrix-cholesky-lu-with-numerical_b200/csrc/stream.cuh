@@ -13,8 +13,8 @@
 // Schedule. A counting sort (histogram, scan, scatter) orders the matrices by
 // bucket = (kind, padded order NP in {8, 16, ..., 64}, right-hand-side class
 // {<= 2, <= 8}); each bucket is cut into work units of S matrices (S = 32/G
-// segments per warp for NP <= 32: 4 up to order 16, 2 up to 32; or one warp per
-// matrix when the tuned schedule asks for it). One persistent launch then drains the units through a global
+// segments per warp for NP <= 32, as unit_size lists; or one warp per matrix when
+// the tuned schedule asks for it). One persistent launch then drains the units through a global
 // atomic queue, largest order first, so at any moment the SMs run mostly the same
 // code variant and the smallest units fill the tail; each unit is the same
 // per-matrix body (blk.cuh) as the dense kernels, so the results are
@@ -57,15 +57,21 @@ __device__ __forceinline__ int bucket_of(int kind, int n, int nrhs) {
   return ((kStreamClasses - 1 - np_class(n)) * 2 + (kind ? 1 : 0)) * 2 + (nrhs > 2 ? 1 : 0);
 }
 __device__ __forceinline__ int bucket_class(int b) { return kStreamClasses - 1 - (b >> 2); }
-// matrices per work unit for a bucket: 4 (n <= 16) or 2 (17 <= n <= 32) segments
-// share a warp unless sched bit c (order class c = 0..3) asks for one matrix per warp
+// matrices per work unit for a bucket (the dense kernels' measured packings): order
+// <= 8: 8 (Cholesky, 4 lanes each) or 4 (LU); order 9..16: 4; order 17..24: 4 in
+// float32, 2 in float64; order 25..32: 2; above: 1. Sched bit c (order class c =
+// 0..3) asks for one matrix per warp instead.
+template <class T>
 __device__ __forceinline__ int unit_size(int b, unsigned sched) {
   const int c = bucket_class(b);
+  const bool lu = (b >> 1) & 1;
   if (c >= 4 || ((sched >> c) & 1u)) return 1;
-  return c <= 1 ? 4 : 2;
+  if (c == 0) return lu ? 4 : 8;
+  if (c == 1) return 4;
+  if (c == 2) return sizeof(T) == 4 ? 4 : 2;
+  return 2;
 }
 
-// Histogram: block-local counts in shared memory, one global atomic per bucket per block.
 template <class T>
 __global__ void stream_hist_kernel(StreamArgs<T> a) {
   __shared__ int h[kStreamBuckets];
@@ -91,7 +97,7 @@ __global__ void stream_scan_kernel(StreamArgs<T> a) {
     cur[b] = s;
     ustart[b] = u;
     s += cnt[b];
-    const int us = unit_size(b, a.sched);
+    const int us = unit_size<T>(b, a.sched);
     u += (cnt[b] + us - 1) / us;
   }
   ustart[kStreamBuckets] = u;
@@ -174,7 +180,7 @@ __global__ void __launch_bounds__(WPC * 32, 1) stream_kernel(StreamArgs<T> a) {
     if (w >= total) break;
     int b = 0;
     while (b + 1 < kStreamBuckets && ustart_s[b + 1] <= w) ++b;
-    const int us = unit_size(b, a.sched);
+    const int us = unit_size<T>(b, a.sched);
     const int first = start[b] + (w - ustart_s[b]) * us;
     const int last = min(first + us, start[b] + cnt[b]);
     const bool one = us == 1;
@@ -188,9 +194,27 @@ __global__ void __launch_bounds__(WPC * 32, 1) stream_kernel(StreamArgs<T> a) {
   if (wide) { TSDX_SU_KIND(NP_, 8, G_); } \
   else { TSDX_SU_KIND(NP_, 2, G_); }
     switch (c) {
-      case 0: if (one) { TSDX_SU_RHS(8, 32) } else { TSDX_SU_RHS(8, 8) } break;
+      case 0:
+        if (one) {
+          TSDX_SU_RHS(8, 32)
+        } else if (wide) {
+          if (lu) TSDX_SU(8, 8, false, 8);
+          else TSDX_SU(8, 8, true, 4);
+        } else {
+          if (lu) TSDX_SU(8, 2, false, 8);
+          else TSDX_SU(8, 2, true, 4);
+        }
+        break;
       case 1: if (one) { TSDX_SU_RHS(16, 32) } else { TSDX_SU_RHS(16, 8) } break;
-      case 2: if (one) { TSDX_SU_RHS(24, 32) } else { TSDX_SU_RHS(24, 16) } break;
+      case 2:
+        if (one) {
+          TSDX_SU_RHS(24, 32)
+        } else if constexpr (sizeof(T) == 4) {
+          TSDX_SU_RHS(24, 8)
+        } else {
+          TSDX_SU_RHS(24, 16)
+        }
+        break;
       case 3: if (one) { TSDX_SU_RHS(32, 32) } else { TSDX_SU_RHS(32, 16) } break;
       case 4: TSDX_SU_RHS(40, 32) break;
       case 5: TSDX_SU_RHS(48, 32) break;

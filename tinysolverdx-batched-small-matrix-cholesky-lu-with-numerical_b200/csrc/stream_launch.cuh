@@ -18,6 +18,7 @@ template <class T> constexpr int stream_warpb() {
   constexpr int w[] = {BlkCfg<T, 8, 8>::WARPB,  BlkCfg<T, 8, 8, 32>::WARPB, BlkCfg<T, 16, 8>::WARPB,
                        BlkCfg<T, 16, 8, 32>::WARPB, BlkCfg<T, 24, 8>::WARPB, BlkCfg<T, 32, 8>::WARPB,
                        BlkCfg<T, 24, 8, 16>::WARPB, BlkCfg<T, 32, 8, 16>::WARPB, BlkCfg<T, 16, 8, 8>::WARPB,
+                       BlkCfg<T, 8, 8, 4>::WARPB, BlkCfg<T, 24, 8, 8>::WARPB,
                        BlkCfg<T, 40, 8>::WARPB, BlkCfg<T, 48, 8>::WARPB, BlkCfg<T, 56, 8>::WARPB,
                        BlkCfg<T, 64, 8>::WARPB};
   int m = 0;

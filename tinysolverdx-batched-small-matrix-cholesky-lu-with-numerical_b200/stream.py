@@ -20,7 +20,8 @@ from . import capi
 
 CHOLESKY, LU = 0, 1
 # sched bit c (order class c: n in 1..8, 9..16, 17..24, 25..32) set -> those matrices
-# run one per warp; clear -> four (classes 0-1) or two (classes 2-3) share a warp
+# run one per warp; clear -> they share a warp (8 Cholesky or 4 LU at n <= 8, 4 at
+# n <= 16, 4 (float32) or 2 (float64) at n <= 24, 2 at n <= 32)
 SCHED_BITS = 4
 
 
