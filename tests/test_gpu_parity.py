@@ -284,8 +284,13 @@ def test_markstein_division(dtype):
                      2.0, 0.5, 3.0, 1.0 - fi.eps / 2, 1.0 + fi.eps, fi.smallest_subnormal], dtype)
     ea, eb = np.meshgrid(edge, edge)
     ones = np.full(m // 4, 1.0, dtype) + rng.integers(0, 1 << 20, m // 4).astype(dtype) * fi.eps  # near-1 divisors
-    a = np.concatenate([a, ea.ravel(), rng.standard_normal(m // 4).astype(dtype)])
-    b = np.concatenate([b, eb.ravel(), ones])
+    # signed zeros over divisors of every magnitude, subnormals included (the rows that
+    # pad a matrix up to its kernel's tile divide zeros at every pivot step)
+    zs = np.where(rng.random(m // 4) < 0.5, 0.0, -0.0).astype(dtype)
+    zd = (rng.standard_normal(m // 4) * 10.0 ** rng.uniform(lo, hi, m // 4)).astype(dtype)
+    zd[::7] = (rng.standard_normal(zd[::7].size) * fi.smallest_subnormal * 1000).astype(dtype)
+    a = np.concatenate([a, ea.ravel(), rng.standard_normal(m // 4).astype(dtype), zs])
+    b = np.concatenate([b, eb.ravel(), ones, zd])
     ta, tb = dev(a), dev(b)
     fast, ieee = torch.empty_like(ta), torch.empty_like(ta)
     name = "tsdx_internal_div_check_" + capi.sfx(np.dtype(dtype))

@@ -44,9 +44,15 @@ __device__ __forceinline__ float sqrt_(float a) { return __fsqrt_rn(a); }
 // RN(q + e*y) = RN(a/b) as long as no intermediate underflows or overflows.
 // A pivot step divides a whole column by one pivot, so y is computed once
 // (__drcp_rn / __frcp_rn, IEEE round-to-nearest) and every quotient costs a
-// multiply and two FMAs. Operands outside the safe range (zeros, subnormals,
-// huge values, Inf, NaN) take the IEEE division. Checked bit-for-bit against
-// __ddiv_rn / __fdiv_rn by tests/test_gpu_parity.py::test_markstein_division.
+// multiply and two FMAs. A zero numerator is answered by q itself whenever q is
+// not NaN: then y is finite, so b is neither zero nor NaN, and a*y is the zero
+// with the sign of a XOR the sign of b (RN(1/b) keeps b's sign, also when it
+// underflows), which is IEEE's a/b. This case is common, not rare: the rows that
+// pad an order up to its kernel's tile are zero left of the diagonal block, so
+// each pivot step divides zeros. Other operands outside the safe range
+// (subnormals, huge values, Inf, NaN, a zero over a zero or a subnormal divisor)
+// take the IEEE division. Checked bit-for-bit against __ddiv_rn / __fdiv_rn by
+// tests/test_gpu_parity.py::test_markstein_division.
 static __device__ __noinline__ double div_slow(double a, double b) { return __ddiv_rn(a, b); }
 static __device__ __noinline__ float div_slow(float a, float b) { return __fdiv_rn(a, b); }
 __device__ __forceinline__ double rcp_(double b) { return __drcp_rn(b); }
@@ -54,14 +60,14 @@ __device__ __forceinline__ float rcp_(float b) { return __frcp_rn(b); }
 __device__ __forceinline__ double div_by(double a, double b, double y) {
   const double q = __dmul_rn(a, y);
   const double aq = fabs(q), aa = fabs(a);
-  if (!(aq >= 0x1p-960 && aq <= 0x1p+960 && aa >= 0x1p-960 && aa <= 0x1p+960)) return div_slow(a, b);
+  if (!(aq >= 0x1p-960 && aq <= 0x1p+960 && aa >= 0x1p-960 && aa <= 0x1p+960)) return (a == 0.0 && q == 0.0) ? q : div_slow(a, b);
   const double e = __fma_rn(-b, q, a);
   return __fma_rn(e, y, q);
 }
 __device__ __forceinline__ float div_by(float a, float b, float y) {
   const float q = __fmul_rn(a, y);
   const float aq = fabsf(q), aa = fabsf(a);
-  if (!(aq >= 0x1p-100f && aq <= 0x1p+100f && aa >= 0x1p-100f && aa <= 0x1p+100f)) return div_slow(a, b);
+  if (!(aq >= 0x1p-100f && aq <= 0x1p+100f && aa >= 0x1p-100f && aa <= 0x1p+100f)) return (a == 0.0f && q == 0.0f) ? q : div_slow(a, b);
   const float e = __fmaf_rn(-b, q, a);
   return __fmaf_rn(e, y, q);
 }
