@@ -190,6 +190,25 @@ int tsdx_cuda_solve_stream_f64(double* A, const int64_t* aoff, double* B, const 
                                const signed char* kind, int64_t count, int write_factors, unsigned sched,
                                void* scratch, int64_t scratch_bytes, void* stream);
 
+/* ---- uneven stream from host memory (no reference counterpart) --------------------
+ * The same solve with A, B, piv and info in HOST memory, packed back to back in index
+ * order: matrix i's A at sum_{j<i} n_j^2 elements, its right-hand sides at
+ * sum_{j<i} n_j*nrhs_j, its pivots at sum_{j<i} n_j (the packing of the Python
+ * layer's stream.layout). n, nrhs and kind are host arrays too. Synchronous, like the
+ * *_batched_host_* calls: the set crosses the device in chunks of about 96 MB of A, so
+ * the device holds three chunks at a time whatever the size of the set, and each
+ * chunk's host->device copy overlaps the previous chunk's solve and the device->host
+ * copy of the one before. The copies overlap only when the host buffers are pinned
+ * (page-locked); pageable buffers work but serialize. Every entry is checked before
+ * any copy: n outside [1, 64] -> TSDX_ERR_N, nrhs outside [0, 8] -> TSDX_ERR_NRHS.
+ * B may be NULL when every nrhs is 0, piv when write_factors is 0; info may be NULL.
+ * The pivot slots of Cholesky matrices come back unchanged.
+ * Factors, pivots, info and X are bit-identical to tsdx_cuda_solve_stream_*. */
+int tsdx_cuda_solve_stream_host_f32(float* A, float* B, int* piv, int* info, const int* n, const int* nrhs,
+                                    const signed char* kind, int64_t count, int write_factors, unsigned sched);
+int tsdx_cuda_solve_stream_host_f64(double* A, double* B, int* piv, int* info, const int* n, const int* nrhs,
+                                    const signed char* kind, int64_t count, int write_factors, unsigned sched);
+
 /* ---- uneven stream without allocation (no reference counterpart) ------------------
  * tsdx_cuda_solve_stream_f32 with the scratch in a fixed 1 MiB (+520 B) device array
  * of the library instead of caller memory: allocates nothing, for callers that may

@@ -53,3 +53,23 @@ def test_stream_validation_without_device():
     assert "262144" in capi.last_error()
     assert lib.tsdx_cuda_solve_stream_noalloc_f32(*nul, -3, 1, 0, None) == capi.TSDX_ERR_BATCH
     assert lib.tsdx_cuda_solve_stream_noalloc_f32(*nul, 0, 1, 0, None) == capi.TSDX_OK
+    # host-memory stream: every entry is checked before any CUDA call
+    import numpy as np
+    nn = np.array([3, 65], np.int32)
+    rr = np.array([1, 1], np.int32)
+    kk = np.zeros(2, np.int8)
+    A = np.zeros(9 + 65 * 65, np.float32)
+    B = np.zeros(3 + 65, np.float32)
+    pv = np.zeros(68, np.int32)
+    f = lib.tsdx_cuda_solve_stream_host_f32
+    P = capi.ptr
+    assert f(P(A), P(B), P(pv), None, P(nn), P(rr), P(kk), 2, 1, 0) == capi.TSDX_ERR_N
+    nn[1] = 2
+    rr[0] = 9
+    assert f(P(A), P(B), P(pv), None, P(nn), P(rr), P(kk), 2, 1, 0) == capi.TSDX_ERR_NRHS
+    rr[0] = 1
+    assert f(P(A), None, P(pv), None, P(nn), P(rr), P(kk), 2, 1, 0) == capi.TSDX_ERR_NULL  # B with nrhs > 0
+    assert f(P(A), P(B), None, None, P(nn), P(rr), P(kk), 2, 1, 0) == capi.TSDX_ERR_NULL  # piv with factors
+    assert f(None, P(B), P(pv), None, P(nn), P(rr), P(kk), 2, 1, 0) == capi.TSDX_ERR_NULL
+    assert lib.tsdx_cuda_solve_stream_host_f64(None, None, None, None, None, None, None, -1, 1, 0) == capi.TSDX_ERR_BATCH
+    assert lib.tsdx_cuda_solve_stream_host_f64(None, None, None, None, None, None, None, 0, 1, 0) == capi.TSDX_OK

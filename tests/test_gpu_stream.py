@@ -180,3 +180,75 @@ def test_numpy_solve_stream():
     assert np.array_equal(X[0], x0) and np.array_equal(X[1], x1)
     LU, piv, _ = tsdx.lu(mats[1], backend="cuda")
     assert np.array_equal(F[1], LU) and np.array_equal(P[1], piv) and P[0] is None
+
+
+def packed_random_stream(seed, count, dtype, nmax=64):
+    """A large packed stream built per order group (SPD M M^T + n I for Cholesky,
+    Gaussian for LU): no per-matrix Python work, so it can span several chunks."""
+    r = np.random.default_rng(seed)
+    n = r.integers(1, nmax + 1, count).astype(np.int32)
+    kind = r.integers(0, 2, count).astype(np.int8)
+    nrhs = r.choice([0, 1, 2, 4, 8], count).astype(np.int32)
+    aoff, boff, _, na, nb, _ = stream.layout(torch.from_numpy(n), torch.from_numpy(nrhs))
+    aoff, boff = aoff.numpy(), boff.numpy()
+    A = np.empty(na, dtype)
+    B = r.standard_normal(max(nb, 1)).astype(dtype)
+    for nn in np.unique(n):
+        idx = np.nonzero(n == nn)[0]
+        G = r.standard_normal((idx.size, nn, nn))
+        S = G @ G.transpose(0, 2, 1) + nn * np.eye(nn)
+        M = np.where((kind[idx] == 0)[:, None, None], S, G).astype(dtype)
+        A[aoff[idx, None] + np.arange(nn * nn)[None, :]] = M.reshape(idx.size, -1)
+    return n, nrhs, kind, torch.from_numpy(A), torch.from_numpy(B)
+
+
+def run_host_call(n, nrhs, kind, A, B, wf=True, sched=0, pin=False, piv_fill=0):
+    _, _, _, na, nb, npv = stream.layout(torch.from_numpy(n), torch.from_numpy(nrhs))
+    A, B = A.clone(), B.clone()
+    piv = torch.full((max(npv, 1),), piv_fill, dtype=torch.int32)
+    info = torch.full((len(n),), 77, dtype=torch.int32)
+    if pin:
+        A, B, piv, info = A.pin_memory(), B.pin_memory(), piv.pin_memory(), info.pin_memory()
+    stream.solve_host(A, B, piv, info, torch.from_numpy(n), torch.from_numpy(nrhs), torch.from_numpy(kind), wf, sched)
+    return A, B, piv, info
+
+
+def check_host_equals_device(host_out, dev_out, wf):
+    hA, hB, hP, hI = host_out
+    dA, dB, dP, dI = (t.cpu() for t in dev_out)
+    assert torch.equal(hI, dI)
+    assert bits_equal(hB, dB)
+    if wf:
+        assert bits_equal(hA, dA) and torch.equal(hP, dP)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("wf,sched", [(True, 0), (False, 15)])
+def test_stream_host_small_pageable(dtype, wf, sched):
+    """Host-memory stream call (one chunk, pageable buffers) == the device stream call."""
+    n, nrhs, kind, mats, bs, A, B = make_stream(41, 300, dtype)
+    check_host_equals_device(run_host_call(n, nrhs, kind, A, B, wf, sched),
+                             run_direct(n, nrhs, kind, A, B, wf, sched), wf)
+    if wf:  # and against the dense kernels directly
+        hA, hB, hP, hI = run_host_call(n, nrhs, kind, A, B, wf, sched)
+        check_against_dense(n, nrhs, kind, dense_reference(n, nrhs, kind, mats, bs, dtype), hA, hB, hP, hI)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_stream_host_many_chunks_pinned(dtype):
+    """A set of several 96 MB chunks from pinned memory: every matrix bit-identical to
+    the single device call over the whole set (chunk boundaries and rebased offsets)."""
+    count = 90_000 if dtype == np.float32 else 45_000  # about 500 MB of A: 5 or 6 chunks
+    n, nrhs, kind, A, B = packed_random_stream(5, count, dtype)
+    assert A.numel() * A.element_size() > 4 * (96 << 20)
+    host = run_host_call(n, nrhs, kind, A, B, True, 0, pin=True, piv_fill=-7)
+    dev_out = run_direct(n, nrhs, kind, A, B, True, 0)
+    # Cholesky matrices get no pivots: their slots keep the caller's -7, the LU slots
+    # match the device call
+    _, _, poff, *_ = stream.layout(torch.from_numpy(n), torch.from_numpy(nrhs))
+    chol = torch.from_numpy(np.repeat(kind == 0, n))
+    assert (host[2][:chol.numel()][chol] == -7).all()
+    dP = dev_out[2].cpu()
+    dP[:chol.numel()][chol] = -7
+    check_host_equals_device(host, (dev_out[0], dev_out[1], dP, dev_out[3]), True)
+    assert (host[3] == 0).mean(dtype=torch.float64) > 0.4  # the SPD half factors (info 0)

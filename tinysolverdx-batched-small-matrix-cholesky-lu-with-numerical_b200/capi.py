@@ -51,6 +51,8 @@ SIGNATURES.update({"tsdx_cuda_available": [], "tsdx_cuda_launch_count": [],
                    "tsdx_cuda_solve_stream_f32": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _I, C.c_uint, _P, _I64, _P],
                    "tsdx_cuda_solve_stream_f64": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _I, C.c_uint, _P, _I64, _P],
                    "tsdx_cuda_solve_stream_noalloc_f32": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _I, C.c_uint, _P],
+                   "tsdx_cuda_solve_stream_host_f32": [_P, _P, _P, _P, _P, _P, _P, _I64, _I, C.c_uint],
+                   "tsdx_cuda_solve_stream_host_f64": [_P, _P, _P, _P, _P, _P, _P, _I64, _I, C.c_uint],
                    "tsdx_cuda_emu_factor_host": [_I, _I, _P, _I, _I64, _P, _P],
                    "tsdx_cuda_emu_solve_host": [_I, _I, _P, _P, _I, _I64, _P, _I],
                    "tsdx_cuda_solve_backward_error_f64": [_P, _P, _P, _I, _I64, _P, _P],

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/tsdx_cuda.h"
 #include "launch.cuh"
@@ -326,6 +327,195 @@ int stream_entry(T* A, const int64_t* aoff, T* B, const int64_t* boff, int* piv,
   if (B && !boff) return TSDX_ERR_NULL;
   return tsdx::host::run_stream<T>(a, scratch, scratch_bytes, ST(st));
 }
+
+// ---- uneven stream from host memory ------------------------------------------------
+// The packed set is cut into chunks of about kChunkBytes of A, in index order. A chunk
+// travels with its own metadata record (offsets rebased to the chunk's first matrix,
+// orders, right-hand-side counts, kinds), so the device holds kSlots chunks at a time
+// whatever the size of the set, and chunk c's host->device copy, chunk c-1's sort and
+// drain and chunk c-2's device->host copy run at the same time on the slots' streams.
+struct StreamSlotWs {
+  void* a = nullptr;
+  void* b = nullptr;
+  int* piv = nullptr;
+  int* info = nullptr;
+  void* meta = nullptr;  // metadata record, then the sort scratch
+  size_t acap = 0, bcap = 0, pcap = 0, icap = 0, mcap = 0;
+};
+struct StreamHostCtx {
+  StreamSlotWs ws[tsdx::host::kSlots];
+  void* hmeta = nullptr;  // pinned: every chunk's metadata record of the current call
+  size_t hcap = 0;
+};
+StreamHostCtx g_stream_ctx[64];
+
+// record of cnt matrices: aoff, boff, poff (int64), n, nrhs (int32), kind (int8)
+constexpr size_t meta_record_bytes(int64_t cnt) { return (size_t(cnt) * 33 + 255) / 256 * 256; }
+
+template <class T>
+int stream_host_entry(T* A, T* B, int* piv, int* info, const int* n, const int* nrhs, const signed char* kind,
+                      int64_t count, int write_factors, unsigned sched) {
+  using tsdx::host::kChunkBytes;
+  using tsdx::host::kSlots;
+  using tsdx::host::set_cuda_error;
+  if (count < 0 || count > (int64_t(1) << 31) - 1) return TSDX_ERR_BATCH;
+  if (count == 0) return TSDX_OK;
+  if (!A || !n || !nrhs || !kind) return TSDX_ERR_NULL;
+  if (write_factors && !piv) return TSDX_ERR_NULL;
+  int64_t na = 0, nb = 0, np = 0;
+  for (int64_t i = 0; i < count; ++i) {
+    if (n[i] < 1 || n[i] > 64) return TSDX_ERR_N;
+    if (nrhs[i] < 0 || nrhs[i] > 8) return TSDX_ERR_NRHS;
+    na += int64_t(n[i]) * n[i];
+    nb += int64_t(n[i]) * nrhs[i];
+    np += n[i];
+  }
+  if (nb > 0 && !B) return TSDX_ERR_NULL;
+  int devi = 0;
+  if (cudaGetDevice(&devi) != cudaSuccess) return TSDX_ERR_NODEV;
+  if (devi >= 64) return TSDX_ERR_NODEV;
+
+  // chunk c: matrices first[c] .. first[c+1]-1 holding ext[c] = {A, B, pivot} elements
+  struct Ext {
+    int64_t a, b, p;
+  };
+  std::vector<int64_t> first;
+  std::vector<Ext> ext;
+  int64_t mx_cnt = 0, mx_a = 0, mx_b = 0, mx_p = 0, meta_total = 0;
+  {
+    int64_t i0 = 0, a = 0, b = 0, p = 0;
+    for (int64_t i = 0; i < count; ++i) {
+      a += int64_t(n[i]) * n[i];
+      b += int64_t(n[i]) * nrhs[i];
+      p += n[i];
+      if (size_t(a) * sizeof(T) >= kChunkBytes || i + 1 == count) {
+        first.push_back(i0);
+        ext.push_back({a, b, p});
+        mx_cnt = std::max(mx_cnt, i + 1 - i0);
+        mx_a = std::max(mx_a, a);
+        mx_b = std::max(mx_b, b);
+        mx_p = std::max(mx_p, p);
+        meta_total += int64_t(meta_record_bytes(i + 1 - i0));
+        i0 = i + 1;
+        a = b = p = 0;
+      }
+    }
+    first.push_back(count);
+  }
+
+  std::lock_guard<std::mutex> lock(tsdx::host::g_host_mu);
+  tsdx::host::DeviceCtx& ctx = tsdx::host::g_ctx[devi];
+  if (!ctx.init) {
+    for (auto& s : ctx.slot) TSDX_CK(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking), "cudaStreamCreate");
+    ctx.init = true;
+  }
+  StreamHostCtx& sc = g_stream_ctx[devi];
+  const size_t scratch_bytes = size_t(tsdx::host::stream_scratch_bytes(mx_cnt));
+  for (auto& w : sc.ws) {
+    using tsdx::host::grow;
+    if (int rc = grow(&w.a, &w.acap, size_t(mx_a) * sizeof(T))) return rc;
+    if (nb > 0)
+      if (int rc = grow(&w.b, &w.bcap, size_t(std::max<int64_t>(mx_b, 1)) * sizeof(T))) return rc;
+    if (write_factors)
+      if (int rc = grow(reinterpret_cast<void**>(&w.piv), &w.pcap, size_t(mx_p) * sizeof(int))) return rc;
+    if (info)
+      if (int rc = grow(reinterpret_cast<void**>(&w.info), &w.icap, size_t(mx_cnt) * sizeof(int))) return rc;
+    if (int rc = grow(&w.meta, &w.mcap, meta_record_bytes(mx_cnt) + scratch_bytes)) return rc;
+  }
+  if (size_t(meta_total) > sc.hcap) {
+    // the previous call synchronized its streams before returning: nothing reads the old buffer
+    if (sc.hmeta) cudaFreeHost(sc.hmeta);
+    sc.hmeta = nullptr;
+    sc.hcap = 0;
+    TSDX_CK(cudaMallocHost(&sc.hmeta, size_t(meta_total)), "cudaMallocHost");
+    sc.hcap = size_t(meta_total);
+  }
+
+  // every chunk's record, written before the first copy is queued
+  const int nchunks = int(first.size()) - 1;
+  {
+    unsigned char* rec = static_cast<unsigned char*>(sc.hmeta);
+    for (int c = 0; c < nchunks; ++c) {
+      const int64_t i0 = first[c], cnt = first[c + 1] - i0;
+      int64_t* ao = reinterpret_cast<int64_t*>(rec);
+      int64_t* bo = ao + cnt;
+      int64_t* po = bo + cnt;
+      int* nn = reinterpret_cast<int*>(po + cnt);
+      int* rr = nn + cnt;
+      signed char* kk = reinterpret_cast<signed char*>(rr + cnt);
+      int64_t a = 0, b = 0, p = 0;
+      for (int64_t j = 0; j < cnt; ++j) {
+        const int64_t i = i0 + j;
+        ao[j] = a;
+        bo[j] = b;
+        po[j] = p;
+        nn[j] = n[i];
+        rr[j] = nrhs[i];
+        kk[j] = kind[i];
+        a += int64_t(n[i]) * n[i];
+        b += int64_t(n[i]) * nrhs[i];
+        p += n[i];
+      }
+      rec += meta_record_bytes(cnt);
+    }
+  }
+
+  auto enqueue = [&]() -> int {
+    const unsigned char* rec = static_cast<const unsigned char*>(sc.hmeta);
+    int64_t a0 = 0, b0 = 0, p0 = 0;
+    for (int c = 0; c < nchunks; ++c) {
+      const int64_t i0 = first[c], cnt = first[c + 1] - i0;
+      const int64_t ca = ext[c].a, cb = ext[c].b, cp = ext[c].p;
+      const StreamSlotWs& w = sc.ws[c % kSlots];
+      const cudaStream_t st = ctx.slot[c % kSlots].st;
+      const size_t rb = meta_record_bytes(cnt);
+      unsigned char* dm = static_cast<unsigned char*>(w.meta);
+      TSDX_CK(cudaMemcpyAsync(dm, rec, size_t(cnt) * 33, cudaMemcpyHostToDevice, st), "H2D stream record");
+      TSDX_CK(cudaMemcpyAsync(w.a, A + a0, size_t(ca) * sizeof(T), cudaMemcpyHostToDevice, st), "H2D A");
+      if (cb > 0) TSDX_CK(cudaMemcpyAsync(w.b, B + b0, size_t(cb) * sizeof(T), cudaMemcpyHostToDevice, st), "H2D B");
+      // the solve writes no pivots for Cholesky matrices: their slots go in and come
+      // back unchanged, as the device call leaves them
+      if (write_factors)
+        TSDX_CK(cudaMemcpyAsync(w.piv, piv + p0, size_t(cp) * sizeof(int), cudaMemcpyHostToDevice, st), "H2D piv");
+      tsdx::dev::StreamArgs<T> s{};
+      s.A = static_cast<T*>(w.a);
+      s.B = cb > 0 ? static_cast<T*>(w.b) : nullptr;
+      s.piv = write_factors ? w.piv : nullptr;
+      s.info = info ? w.info : nullptr;
+      s.aoff = reinterpret_cast<const long long*>(dm);
+      s.boff = s.aoff + cnt;
+      s.poff = s.boff + cnt;
+      s.n = reinterpret_cast<const int*>(s.poff + cnt);
+      s.nrhs = s.n + cnt;
+      s.kind = reinterpret_cast<const signed char*>(s.nrhs + cnt);
+      s.count = int(cnt);
+      s.wf = write_factors ? 1 : 0;
+      s.sched = sched;
+      if (int rc = tsdx::host::run_stream<T>(s, dm + rb, (long long)scratch_bytes, st)) return rc;
+      if (write_factors) {
+        TSDX_CK(cudaMemcpyAsync(A + a0, w.a, size_t(ca) * sizeof(T), cudaMemcpyDeviceToHost, st), "D2H A");
+        TSDX_CK(cudaMemcpyAsync(piv + p0, w.piv, size_t(cp) * sizeof(int), cudaMemcpyDeviceToHost, st), "D2H piv");
+      }
+      if (cb > 0) TSDX_CK(cudaMemcpyAsync(B + b0, w.b, size_t(cb) * sizeof(T), cudaMemcpyDeviceToHost, st), "D2H B");
+      if (info) TSDX_CK(cudaMemcpyAsync(info + i0, w.info, size_t(cnt) * sizeof(int), cudaMemcpyDeviceToHost, st), "D2H info");
+      rec += rb;
+      a0 += ca;
+      b0 += cb;
+      p0 += cp;
+    }
+    return TSDX_OK;
+  };
+  // drain the slots' streams on failure too: no copy into the caller's buffers outlives the call
+  int rc = enqueue();
+  for (auto& sl : ctx.slot) {
+    const cudaError_t e = cudaStreamSynchronize(sl.st);
+    if (e != cudaSuccess && rc == TSDX_OK) {
+      set_cuda_error(e, "cudaStreamSynchronize");
+      rc = TSDX_ERR_CUDA;
+    }
+  }
+  return rc;
+}
 }  // namespace
 API int tsdx_cuda_solve_stream_f32(float* A, const int64_t* aoff, float* B, const int64_t* boff, int* piv,
                                    const int64_t* poff, int* info, const int* n, const int* nrhs,
@@ -340,6 +530,14 @@ API int tsdx_cuda_solve_stream_f64(double* A, const int64_t* aoff, double* B, co
                                    void* scratch, int64_t scratch_bytes, void* stream) {
   return stream_entry<double>(A, aoff, B, boff, piv, poff, info, n, nrhs, kind, count, write_factors, sched, scratch,
                               scratch_bytes, stream);
+}
+API int tsdx_cuda_solve_stream_host_f32(float* A, float* B, int* piv, int* info, const int* n, const int* nrhs,
+                                        const signed char* kind, int64_t count, int write_factors, unsigned sched) {
+  return stream_host_entry<float>(A, B, piv, info, n, nrhs, kind, count, write_factors, sched);
+}
+API int tsdx_cuda_solve_stream_host_f64(double* A, double* B, int* piv, int* info, const int* n, const int* nrhs,
+                                        const signed char* kind, int64_t count, int write_factors, unsigned sched) {
+  return stream_host_entry<double>(A, B, piv, info, n, nrhs, kind, count, write_factors, sched);
 }
 
 #define TSDX_DEFINE(T, S)                                                                                      \

@@ -88,6 +88,44 @@ def solve(A, aoff, B, boff, piv, poff, info, n, nrhs, kind, write_factors=True, 
                          capi.stream_ptr(stream)), name)
 
 
+def _check_host(t, name, dtype=None):
+    if t is None:
+        return
+    if t.is_cuda or not t.is_contiguous():
+        raise ValueError(f"{name} must be a contiguous CPU tensor")
+    if dtype is not None and t.dtype != dtype:
+        raise TypeError(f"{name} must be {dtype}, not {t.dtype}")
+
+
+def solve_host(A, B, piv, info, n, nrhs, kind, write_factors=True, sched=0):
+    """Solve a packed stream held in host memory, in place (synchronous).
+
+    Same arguments as ``solve`` without the offsets, all CPU tensors: the matrices
+    are packed back to back in index order (``layout``'s offsets). The library moves
+    the set through the device in chunks of about 96 MB of A with the copies of one
+    chunk overlapping the solve of the next, so the device never holds the whole set.
+    Pin A, B, piv and info (``tensor.pin_memory()``) for the copies to overlap.
+    Raises on n outside [1, 64] or nrhs outside [0, 8] before anything is copied.
+    """
+    _check_host(A, "A")
+    if A.dtype not in (torch.float32, torch.float64):
+        raise TypeError("A must be float32 or float64")
+    _check_host(B, "B", A.dtype)
+    for t, nm in ((piv, "piv"), (info, "info"), (n, "n"), (nrhs, "nrhs")):
+        _check_host(t, nm, torch.int32)
+    _check_host(kind, "kind", torch.int8)
+    count = n.numel()
+    if nrhs.numel() != count or kind.numel() != count or (info is not None and info.numel() < count):
+        raise ValueError("n, nrhs, kind and info must have one entry per matrix")
+    _, _, _, na, nb, npv = layout(n, nrhs)
+    if A.numel() < na or (nb and (B is None or B.numel() < nb)) or (write_factors and (piv is None or piv.numel() < npv)):
+        raise ValueError("A, B or piv smaller than the packed layout of n and nrhs")
+    name = f"tsdx_cuda_solve_stream_host_{capi.sfx(A.dtype)}"
+    P = capi.ptr
+    capi.check(capi.call(name, P(A), P(B), P(piv), P(info), P(n), P(nrhs), P(kind), count,
+                         int(bool(write_factors)), int(sched)), name)
+
+
 class StreamPlan:
     """A fixed stream layout with device buffers, a tuned schedule and a CUDA graph.
 
