@@ -329,11 +329,17 @@ int stream_entry(T* A, const int64_t* aoff, T* B, const int64_t* boff, int* piv,
 }
 
 // ---- uneven stream from host memory ------------------------------------------------
-// The packed set is cut into chunks of about kChunkBytes of A, in index order. A chunk
-// travels with its own metadata record (offsets rebased to the chunk's first matrix,
-// orders, right-hand-side counts, kinds), so the device holds kSlots chunks at a time
-// whatever the size of the set, and chunk c's host->device copy, chunk c-1's sort and
-// drain and chunk c-2's device->host copy run at the same time on the slots' streams.
+// The packed set is cut into chunks of about kStreamChunkBytes of A, in index order. A
+// chunk travels with its own metadata record (offsets rebased to the chunk's first
+// matrix, orders, right-hand-side counts, kinds), so the device holds kStreamSlots
+// chunks at a time whatever the size of the set, and chunk c's host->device copy,
+// chunk c-1's sort and drain and chunk c-2's device->host copy run at the same time on
+// the slots' streams. One host pass validates every entry and cuts the chunks before
+// anything is copied; each chunk's record is written just before its copies are
+// queued, while the earlier chunks are in flight.
+constexpr int kStreamSlots = 3;
+constexpr size_t kStreamChunkBytes = size_t(96) << 20;
+
 struct StreamSlotWs {
   void* a = nullptr;
   void* b = nullptr;
@@ -341,9 +347,11 @@ struct StreamSlotWs {
   int* info = nullptr;
   void* meta = nullptr;  // metadata record, then the sort scratch
   size_t acap = 0, bcap = 0, pcap = 0, icap = 0, mcap = 0;
+  cudaStream_t st = nullptr;
 };
 struct StreamHostCtx {
-  StreamSlotWs ws[tsdx::host::kSlots];
+  StreamSlotWs ws[kStreamSlots];
+  bool init = false;
   void* hmeta = nullptr;  // pinned: every chunk's metadata record of the current call
   size_t hcap = 0;
 };
@@ -355,25 +363,11 @@ constexpr size_t meta_record_bytes(int64_t cnt) { return (size_t(cnt) * 33 + 255
 template <class T>
 int stream_host_entry(T* A, T* B, int* piv, int* info, const int* n, const int* nrhs, const signed char* kind,
                       int64_t count, int write_factors, unsigned sched) {
-  using tsdx::host::kChunkBytes;
-  using tsdx::host::kSlots;
   using tsdx::host::set_cuda_error;
   if (count < 0 || count > (int64_t(1) << 31) - 1) return TSDX_ERR_BATCH;
   if (count == 0) return TSDX_OK;
   if (!A || !n || !nrhs || !kind) return TSDX_ERR_NULL;
   if (write_factors && !piv) return TSDX_ERR_NULL;
-  int64_t na = 0, nb = 0, np = 0;
-  for (int64_t i = 0; i < count; ++i) {
-    if (n[i] < 1 || n[i] > 64) return TSDX_ERR_N;
-    if (nrhs[i] < 0 || nrhs[i] > 8) return TSDX_ERR_NRHS;
-    na += int64_t(n[i]) * n[i];
-    nb += int64_t(n[i]) * nrhs[i];
-    np += n[i];
-  }
-  if (nb > 0 && !B) return TSDX_ERR_NULL;
-  int devi = 0;
-  if (cudaGetDevice(&devi) != cudaSuccess) return TSDX_ERR_NODEV;
-  if (devi >= 64) return TSDX_ERR_NODEV;
 
   // chunk c: matrices first[c] .. first[c+1]-1 holding ext[c] = {A, B, pivot} elements
   struct Ext {
@@ -382,19 +376,24 @@ int stream_host_entry(T* A, T* B, int* piv, int* info, const int* n, const int* 
   std::vector<int64_t> first;
   std::vector<Ext> ext;
   int64_t mx_cnt = 0, mx_a = 0, mx_b = 0, mx_p = 0, meta_total = 0;
+  bool any_b = false;
   {
     int64_t i0 = 0, a = 0, b = 0, p = 0;
     for (int64_t i = 0; i < count; ++i) {
-      a += int64_t(n[i]) * n[i];
-      b += int64_t(n[i]) * nrhs[i];
-      p += n[i];
-      if (size_t(a) * sizeof(T) >= kChunkBytes || i + 1 == count) {
+      const int ni = n[i], ri = nrhs[i];
+      if (ni < 1 || ni > 64) return TSDX_ERR_N;
+      if (ri < 0 || ri > 8) return TSDX_ERR_NRHS;
+      a += int64_t(ni) * ni;
+      b += int64_t(ni) * ri;
+      p += ni;
+      if (size_t(a) * sizeof(T) >= kStreamChunkBytes || i + 1 == count) {
         first.push_back(i0);
         ext.push_back({a, b, p});
         mx_cnt = std::max(mx_cnt, i + 1 - i0);
         mx_a = std::max(mx_a, a);
         mx_b = std::max(mx_b, b);
         mx_p = std::max(mx_p, p);
+        any_b = any_b || b > 0;
         meta_total += int64_t(meta_record_bytes(i + 1 - i0));
         i0 = i + 1;
         a = b = p = 0;
@@ -402,20 +401,23 @@ int stream_host_entry(T* A, T* B, int* piv, int* info, const int* n, const int* 
     }
     first.push_back(count);
   }
+  if (any_b && !B) return TSDX_ERR_NULL;
+  int devi = 0;
+  if (cudaGetDevice(&devi) != cudaSuccess) return TSDX_ERR_NODEV;
+  if (devi >= 64) return TSDX_ERR_NODEV;
 
   std::lock_guard<std::mutex> lock(tsdx::host::g_host_mu);
-  tsdx::host::DeviceCtx& ctx = tsdx::host::g_ctx[devi];
-  if (!ctx.init) {
-    for (auto& s : ctx.slot) TSDX_CK(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking), "cudaStreamCreate");
-    ctx.init = true;
-  }
   StreamHostCtx& sc = g_stream_ctx[devi];
+  if (!sc.init) {
+    for (auto& w : sc.ws) TSDX_CK(cudaStreamCreateWithFlags(&w.st, cudaStreamNonBlocking), "cudaStreamCreate");
+    sc.init = true;
+  }
   const size_t scratch_bytes = size_t(tsdx::host::stream_scratch_bytes(mx_cnt));
   for (auto& w : sc.ws) {
     using tsdx::host::grow;
     if (int rc = grow(&w.a, &w.acap, size_t(mx_a) * sizeof(T))) return rc;
-    if (nb > 0)
-      if (int rc = grow(&w.b, &w.bcap, size_t(std::max<int64_t>(mx_b, 1)) * sizeof(T))) return rc;
+    if (any_b)
+      if (int rc = grow(&w.b, &w.bcap, size_t(mx_b) * sizeof(T))) return rc;
     if (write_factors)
       if (int rc = grow(reinterpret_cast<void**>(&w.piv), &w.pcap, size_t(mx_p) * sizeof(int))) return rc;
     if (info)
@@ -431,43 +433,37 @@ int stream_host_entry(T* A, T* B, int* piv, int* info, const int* n, const int* 
     sc.hcap = size_t(meta_total);
   }
 
-  // every chunk's record, written before the first copy is queued
   const int nchunks = int(first.size()) - 1;
-  {
-    unsigned char* rec = static_cast<unsigned char*>(sc.hmeta);
-    for (int c = 0; c < nchunks; ++c) {
-      const int64_t i0 = first[c], cnt = first[c + 1] - i0;
-      int64_t* ao = reinterpret_cast<int64_t*>(rec);
-      int64_t* bo = ao + cnt;
-      int64_t* po = bo + cnt;
-      int* nn = reinterpret_cast<int*>(po + cnt);
-      int* rr = nn + cnt;
-      signed char* kk = reinterpret_cast<signed char*>(rr + cnt);
-      int64_t a = 0, b = 0, p = 0;
-      for (int64_t j = 0; j < cnt; ++j) {
-        const int64_t i = i0 + j;
-        ao[j] = a;
-        bo[j] = b;
-        po[j] = p;
-        nn[j] = n[i];
-        rr[j] = nrhs[i];
-        kk[j] = kind[i];
-        a += int64_t(n[i]) * n[i];
-        b += int64_t(n[i]) * nrhs[i];
-        p += n[i];
-      }
-      rec += meta_record_bytes(cnt);
-    }
-  }
-
   auto enqueue = [&]() -> int {
-    const unsigned char* rec = static_cast<const unsigned char*>(sc.hmeta);
+    unsigned char* rec = static_cast<unsigned char*>(sc.hmeta);
     int64_t a0 = 0, b0 = 0, p0 = 0;
     for (int c = 0; c < nchunks; ++c) {
       const int64_t i0 = first[c], cnt = first[c + 1] - i0;
       const int64_t ca = ext[c].a, cb = ext[c].b, cp = ext[c].p;
-      const StreamSlotWs& w = sc.ws[c % kSlots];
-      const cudaStream_t st = ctx.slot[c % kSlots].st;
+      // this chunk's record, in its own region of the pinned buffer
+      {
+        int64_t* ao = reinterpret_cast<int64_t*>(rec);
+        int64_t* bo = ao + cnt;
+        int64_t* po = bo + cnt;
+        int* nn = reinterpret_cast<int*>(po + cnt);
+        int* rr = nn + cnt;
+        signed char* kk = reinterpret_cast<signed char*>(rr + cnt);
+        int64_t a = 0, b = 0, p = 0;
+        for (int64_t j = 0; j < cnt; ++j) {
+          const int ni = n[i0 + j], ri = nrhs[i0 + j];
+          ao[j] = a;
+          bo[j] = b;
+          po[j] = p;
+          nn[j] = ni;
+          rr[j] = ri;
+          kk[j] = kind[i0 + j];
+          a += int64_t(ni) * ni;
+          b += int64_t(ni) * ri;
+          p += ni;
+        }
+      }
+      const StreamSlotWs& w = sc.ws[c % kStreamSlots];
+      const cudaStream_t st = w.st;
       const size_t rb = meta_record_bytes(cnt);
       unsigned char* dm = static_cast<unsigned char*>(w.meta);
       TSDX_CK(cudaMemcpyAsync(dm, rec, size_t(cnt) * 33, cudaMemcpyHostToDevice, st), "H2D stream record");
@@ -497,7 +493,8 @@ int stream_host_entry(T* A, T* B, int* piv, int* info, const int* n, const int* 
         TSDX_CK(cudaMemcpyAsync(piv + p0, w.piv, size_t(cp) * sizeof(int), cudaMemcpyDeviceToHost, st), "D2H piv");
       }
       if (cb > 0) TSDX_CK(cudaMemcpyAsync(B + b0, w.b, size_t(cb) * sizeof(T), cudaMemcpyDeviceToHost, st), "D2H B");
-      if (info) TSDX_CK(cudaMemcpyAsync(info + i0, w.info, size_t(cnt) * sizeof(int), cudaMemcpyDeviceToHost, st), "D2H info");
+      if (info)
+        TSDX_CK(cudaMemcpyAsync(info + i0, w.info, size_t(cnt) * sizeof(int), cudaMemcpyDeviceToHost, st), "D2H info");
       rec += rb;
       a0 += ca;
       b0 += cb;
@@ -507,8 +504,8 @@ int stream_host_entry(T* A, T* B, int* piv, int* info, const int* n, const int* 
   };
   // drain the slots' streams on failure too: no copy into the caller's buffers outlives the call
   int rc = enqueue();
-  for (auto& sl : ctx.slot) {
-    const cudaError_t e = cudaStreamSynchronize(sl.st);
+  for (auto& w : sc.ws) {
+    const cudaError_t e = cudaStreamSynchronize(w.st);
     if (e != cudaSuccess && rc == TSDX_OK) {
       set_cuda_error(e, "cudaStreamSynchronize");
       rc = TSDX_ERR_CUDA;
