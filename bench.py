@@ -516,10 +516,11 @@ def _emit(a, world, value, ms, dt, cfg, roof, cpu, e2e, clk, launches, extra=Non
 
 
 def _link(e2e):
-    """Attach the host link's ceiling to an e2e record. The ceiling is the
-    per-direction rate of pinned host<->device copies of 1 GiB running both ways at
-    once (what a step whose copies in and out overlap can reach); achieved is the
-    step's larger direction over its time."""
+    """Attach the host link's ceiling to an e2e record. Pinned host<->device copies
+    of 1 GiB are timed host->device alone, device->host alone and both ways at once.
+    The ceiling of a step that moves h bytes in and d bytes out, copies overlapped,
+    is min(h, d) at the two-way rate plus the rest of the larger direction at its
+    one-way rate; frac = that time over the step's time."""
     if not e2e or not e2e.get("ms_per_step"):
         return e2e
     import torch
@@ -530,28 +531,39 @@ def _link(e2e):
     d_out = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
     s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
     cur = torch.cuda.current_stream()
-    best = float("inf")
-    for r in range(4):
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(cur)
-        s1.wait_event(e0)
-        s2.wait_event(e0)
-        with torch.cuda.stream(s1):
-            d_in.copy_(h_in, non_blocking=True)
-        with torch.cuda.stream(s2):
-            h_out.copy_(d_out, non_blocking=True)
-        cur.wait_stream(s1)
-        cur.wait_stream(s2)
-        e1.record(cur)
-        e1.synchronize()
-        if r:
-            best = min(best, e0.elapsed_time(e1))
-    peak = nbytes / (best * 1e-3) / 1e9
-    ach = max(e2e["h2d_bytes_per_step"], e2e["d2h_bytes_per_step"]) / (e2e["ms_per_step"] * 1e-3) / 1e9
-    e2e["link"] = {"bound": "pcie", "achieved": round(ach, 1), "peak": round(peak, 1), "unit": "GB/s per direction",
-                   "frac": round(ach / peak, 3),
-                   "peak_how": "pinned host<->device copies of 1 GiB both ways at once, best of 3, CUDA events"}
+
+    def rate(up, down):
+        best = float("inf")
+        for r in range(4):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(cur)
+            s1.wait_event(e0)
+            s2.wait_event(e0)
+            if up:
+                with torch.cuda.stream(s1):
+                    d_in.copy_(h_in, non_blocking=True)
+            if down:
+                with torch.cuda.stream(s2):
+                    h_out.copy_(d_out, non_blocking=True)
+            cur.wait_stream(s1)
+            cur.wait_stream(s2)
+            e1.record(cur)
+            e1.synchronize()
+            if r:
+                best = min(best, e0.elapsed_time(e1))
+        return nbytes / (best * 1e-3) / 1e9
+
+    r_up, r_down, r_both = rate(True, False), rate(False, True), rate(True, True)
+    h, d = e2e["h2d_bytes_per_step"], e2e["d2h_bytes_per_step"]
+    ceil_s = min(h, d) / (r_both * 1e9) + (h - d) / (r_up * 1e9) if h >= d else \
+        min(h, d) / (r_both * 1e9) + (d - h) / (r_down * 1e9)
+    ach = max(h, d) / (e2e["ms_per_step"] * 1e-3) / 1e9
+    e2e["link"] = {"bound": "pcie", "achieved": round(ach, 1), "unit": "GB/s (larger direction)",
+                   "h2d_alone": round(r_up, 1), "d2h_alone": round(r_down, 1), "both_ways": round(r_both, 1),
+                   "ceiling_ms": round(ceil_s * 1e3, 3), "frac": round(ceil_s * 1e3 / e2e["ms_per_step"], 3),
+                   "how": "pinned host<->device copies of 1 GiB: host->device alone, device->host alone, both "
+                          "ways at once (GB/s per direction), best of 3, CUDA events"}
     return e2e
 
 
@@ -572,6 +584,27 @@ def _selector(device):
     if not w.exists():
         raise RuntimeError(f"{w} is missing: train it with {PKG_NAME}/selector_train.py")
     return sel.Selector.load(str(w), device=device)
+
+
+E2E_SELECTOR_API = ("Selector.solve_host (features + tier + tsdx_cuda_*_ir_f64 per 96 MB chunk on 3 streams), "
+                    "pinned host; x, info, status and tier back")
+
+
+def _e2e_selector(s, parts, world, device, dist):
+    """Mean time (ms, max over ranks) of Selector.solve_host over device-resident
+    parts [(A, b, spd)] staged once into pinned host memory; b is restored between
+    steps outside the timed region."""
+    import torch
+    hp = [(A.cpu().pin_memory(), b.cpu().pin_memory(), spd) for A, b, spd in parts]
+    work = [(hA, torch.empty_like(hb).pin_memory(), spd) for hA, hb, spd in hp]
+    ts = []
+    for r in range(4):  # the first call warms the caching allocator
+        for (_, hb, _), (_, wb, _) in zip(hp, work):
+            wb.copy_(hb)
+        t = _once(lambda: s.solve_host(work))
+        if r:
+            ts.append(t)
+    return _max_over_ranks(sum(ts) / len(ts), world, device, dist)
 
 
 def _ir_workload(a, world, rank, local, device, dist):
@@ -639,25 +672,10 @@ def _ir_workload(a, world, rank, local, device, dist):
     # end to end: pinned host A and b in, x and info out, every step
     e2e = None
     if not a.skip_e2e:
-        hp = [(spd, A.cpu().pin_memory(), b.cpu().pin_memory()) for spd, A, b in parts]
-        dA = [torch.empty_like(A) for _, A, _ in parts]
-        dx = [torch.empty_like(b) for _, _, b in parts]
-        hx = [torch.empty(b.shape, dtype=b.dtype, pin_memory=True) for _, _, b in parts]
-        hi = [torch.empty(b.shape[0], dtype=torch.int32, pin_memory=True) for _, _, b in parts]
-
-        def e2e_step():
-            for (spd, hA, hb), A_, x_, hx_, hi_ in zip(hp, dA, dx, hx, hi):
-                A_.copy_(hA, non_blocking=True)
-                x_.copy_(hb, non_blocking=True)
-                info, _, _, _ = s.solve(A_, x_, spd)
-                hx_.copy_(x_, non_blocking=True)
-                hi_.copy_(info, non_blocking=True)
-        e2e_step()
-        t = min(_once(e2e_step) for _ in range(3))
-        t = _max_over_ranks(t, world, device, dist)
+        t = _e2e_selector(s, [(A, b, spd) for spd, A, b in parts], world, device, dist)
         e2e = {"value": round(world * batch / (t * 1e-3), 1), "unit": "solves/s",
-               "h2d_bytes_per_step": batch * (n * n + n) * 8, "d2h_bytes_per_step": batch * (n * 8 + 4),
-               "ms_per_step": round(t, 3), "api": "Selector.solve (features + tier + tsdx_cuda_*_ir_f64), pinned host"}
+               "h2d_bytes_per_step": batch * (n * n + n) * 8, "d2h_bytes_per_step": batch * (n * 8 + 9),
+               "ms_per_step": round(t, 3), "api": E2E_SELECTOR_API}
     cpu = None
     if rank == 0 and world == 1 and not a.skip_cpu:
         rng = np.random.default_rng(5)
@@ -839,7 +857,14 @@ def _selector_workload(a, world, rank, local, device, dist):
     cfg = {"workload": SPECIAL["selector"], "global_batch": world * count, "batch_per_gpu": count,
            "parallelism": f"evaluation set sharded over {world} GPU(s), no collective",
            "l2": "inputs larger than L2 (13 GB of A per step)", "selector": f"{PKG_NAME}/selector_weights.npz"}
-    return value, ms, "f64 (tiers fp16/bf16/fp32 factor, fp64 residual)", cfg, roof, None, None, clk, launches, extra
+    e2e = None
+    if not a.skip_e2e:
+        t = _e2e_selector(s, [(gr["A"], gr["b"], gr["spd"]) for gr in groups], world, device, dist)
+        e2e = {"value": round(world * count / (t * 1e-3), 1), "unit": "solves/s",
+               "h2d_bytes_per_step": sum(gr["count"] * (gr["n"] ** 2 + gr["n"]) * 8 for gr in groups),
+               "d2h_bytes_per_step": sum(gr["count"] * (gr["n"] * 8 + 9) for gr in groups),
+               "ms_per_step": round(t, 3), "api": E2E_SELECTOR_API}
+    return value, ms, "f64 (tiers fp16/bf16/fp32 factor, fp64 residual)", cfg, roof, None, e2e, clk, launches, extra
 
 
 def _ir_fixed_workload(a, world, rank, local, device, dist):

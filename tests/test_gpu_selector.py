@@ -116,3 +116,33 @@ def test_training_learns_and_beats_the_method_without_it(oracle):
     print(f"selector: {miss_sel} misses, {lowprec} refined; fp16-first: {miss_fixed} misses")
     assert miss_sel < 0.5 * miss_fixed
     assert lowprec > 0
+
+
+@pytest.mark.parametrize("shipped", [True, False])
+def test_solve_host_matches_device_solve(shipped):
+    """Selector.solve_host (host buffers, chunks pipelined over 3 streams, several parts)
+    returns x, info, status and tier bit-identical to the device solve of each whole part.
+    shipped: the committed weights and cost table (every order routed to fp64); else an
+    untrained network without costs, so predicted tiers, refinement and fallbacks all run."""
+    import pathlib
+    s = (sel.Selector.load(str(pathlib.Path(sel.__file__).parent / "selector_weights.npz")) if shipped
+         else sel.Selector(seed=3))
+    parts, ref = [], []
+    for i, (n, spd, batch) in enumerate([(64, False, 40), (17, True, 300), (5, False, 7), (64, True, 0)]):
+        A, b = stack(900 + i, max(batch, 1), n, spd, 1.0, 1e12)
+        A, b = A[:batch], b[:batch]
+        Ad, bd = torch.from_numpy(A).cuda(), torch.from_numpy(b).cuda()
+        if batch:
+            info, status, _, tier = s.solve(Ad, bd, spd)
+        else:
+            info = status = torch.zeros(0, dtype=torch.int32)
+            tier = torch.zeros(0, dtype=torch.int8)
+        ref.append((bd.cpu(), info.cpu(), status.cpu(), tier.cpu()))
+        hA = torch.from_numpy(np.ascontiguousarray(A))
+        parts.append((hA.pin_memory() if i % 2 == 0 else hA, torch.from_numpy(np.ascontiguousarray(b)), spd))
+    outs = s.solve_host(parts, chunk_bytes=64 * 64 * 8 * 3)  # 3 matrices of order 64 per chunk
+    for (_, hb, _), (info, status, tier), (x, i0, s0, t0) in zip(parts, outs, ref):
+        assert torch.equal(hb.view(torch.int64), x.view(torch.int64))
+        assert torch.equal(info, i0) and torch.equal(status, s0) and torch.equal(tier, t0)
+    if not shipped:
+        assert int((ref[0][3] < 3).sum()) > 0  # lower tiers did run

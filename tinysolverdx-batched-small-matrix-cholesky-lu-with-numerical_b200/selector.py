@@ -209,3 +209,57 @@ class Selector:
         tier = torch.from_numpy(lut).to(A.device)[self.predict(X).long()].contiguous()
         info, status, bwd = device.ir(A, b, spd, tier=tier, itmax=itmax, tol=tol)
         return info, status, bwd, tier
+
+    def solve_host(self, parts, itmax=3, tol=1e-15, chunk_bytes=96 << 20, slots=3):
+        """``solve`` on batches held in host memory, with the copies overlapping the solves.
+
+        parts: list of (A, b, spd): A (batch, n, n) and b (batch, n) contiguous float64
+        CPU tensors, spd a bool; b is overwritten by x. Pin A and b
+        (``tensor.pin_memory()``) for the copies to overlap. Every part is cut into
+        chunks of about ``chunk_bytes`` of A, and chunk c runs on stream c % slots as
+        host->device copy, ``solve``, device->host copy, so the copies of one chunk
+        overlap the solves of its neighbours, across parts too. The device holds
+        ``slots`` chunks at a time. Returns one (info, status, tier) triple of CPU
+        tensors per part; synchronous."""
+        outs, jobs = [], []
+        for A, b, spd in parts:
+            for t, nm in ((A, "A"), (b, "b")):
+                if t.is_cuda or not t.is_contiguous() or t.dtype != torch.float64:
+                    raise ValueError(f"{nm} must be a contiguous float64 CPU tensor")
+            if A.dim() != 3 or A.shape[1] != A.shape[2] or tuple(b.shape) != (A.shape[0], A.shape[1]):
+                raise ValueError("A must be (batch, n, n) and b (batch, n)")
+            batch, n = A.shape[0], A.shape[-1]
+            pin = A.is_pinned()
+            out = (torch.empty(batch, dtype=torch.int32, pin_memory=pin),
+                   torch.empty(batch, dtype=torch.int32, pin_memory=pin),
+                   torch.empty(batch, dtype=torch.int8, pin_memory=pin))
+            outs.append(out)
+            per = max(1, chunk_bytes // (n * n * 8))
+            jobs += [(A, b, bool(spd), n, i0, min(batch, i0 + per), out) for i0 in range(0, batch, per)]
+        if not jobs:
+            return outs
+        cur = torch.cuda.current_stream(self.device)
+        mA = max((i1 - i0) * n * n for _, _, _, n, i0, i1, _ in jobs)
+        mx = max((i1 - i0) * n for _, _, _, n, i0, i1, _ in jobs)
+        bufA = [torch.empty(mA, dtype=torch.float64, device=self.device) for _ in range(slots)]
+        bufx = [torch.empty(mx, dtype=torch.float64, device=self.device) for _ in range(slots)]
+        streams = [torch.cuda.Stream(self.device) for _ in range(slots)]
+        for st in streams:
+            st.wait_stream(cur)  # the slot buffers were allocated on the current stream
+        for c, (A, b, spd, n, i0, i1, (info, status, tier)) in enumerate(jobs):
+            k, cnt = c % slots, i1 - i0
+            # slot k's buffers are reused by chunk c + slots on the same stream, after
+            # this chunk's copies back; the solve's own temporaries live on that stream too
+            with torch.cuda.stream(streams[k]):
+                dA = bufA[k][:cnt * n * n].view(cnt, n, n)
+                dx = bufx[k][:cnt * n].view(cnt, n)
+                dA.copy_(A[i0:i1], non_blocking=True)
+                dx.copy_(b[i0:i1], non_blocking=True)
+                inf, stt, _, tr = self.solve(dA, dx, spd, itmax=itmax, tol=tol)
+                b[i0:i1].copy_(dx, non_blocking=True)
+                info[i0:i1].copy_(inf, non_blocking=True)
+                status[i0:i1].copy_(stt, non_blocking=True)
+                tier[i0:i1].copy_(tr, non_blocking=True)
+        for st in streams:
+            st.synchronize()
+        return outs
