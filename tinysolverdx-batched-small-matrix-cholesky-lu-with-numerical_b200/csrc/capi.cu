@@ -110,7 +110,11 @@ int run_device(Kind kind, T* A, const int* piv_in, int n, int64_t batch, T* B, i
 
 // ---- host-pointer implementation ----------------------------------------------
 constexpr int kSlots = 3;
-constexpr size_t kChunkBytes = size_t(96) << 20;  // A bytes per chunk
+constexpr size_t kChunkBytes = size_t(96) << 20;  // A bytes per chunk, at most
+// A small batch is still cut into kMinChunks chunks (of at least kMinChunkBytes), so
+// that its copies overlap too: with two chunks, most of the transfer would run alone.
+constexpr int kMinChunks = 8;
+constexpr size_t kMinChunkBytes = size_t(4) << 20;
 
 struct Slot {
   void* a = nullptr;
@@ -168,7 +172,8 @@ int run_host(Kind kind, T* A, const int* piv_in, int n, int64_t batch, T* B, int
     ctx.init = true;
   }
   const size_t mat = size_t(n) * n * sizeof(T), rhs = size_t(n) * nrhs * sizeof(T);
-  const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(batch, int64_t(kChunkBytes / mat)));
+  const size_t target = std::min(kChunkBytes, std::max(kMinChunkBytes, mat * size_t(batch) / kMinChunks));
+  const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(batch, int64_t(target / mat)));
   for (auto& s : ctx.slot) {
     if (int rc = grow(&s.a, &s.acap, mat * chunk)) return rc;
     if (has_b && nrhs > 0)
