@@ -73,3 +73,32 @@ def test_stream_validation_without_device():
     assert f(None, P(B), P(pv), None, P(nn), P(rr), P(kk), 2, 1, 0) == capi.TSDX_ERR_NULL
     assert lib.tsdx_cuda_solve_stream_host_f64(None, None, None, None, None, None, None, -1, 1, 0) == capi.TSDX_ERR_BATCH
     assert lib.tsdx_cuda_solve_stream_host_f64(None, None, None, None, None, None, None, 0, 1, 0) == capi.TSDX_OK
+
+
+def test_stream_solve_host_python_validation():
+    """stream.solve_host rejects device tensors, wrong dtypes and buffers smaller than
+    the packed layout before calling the library; valid empty input is a no-op."""
+    import pytest
+    torch = pytest.importorskip("torch")
+    stream = load_pkg("stream")
+    n = torch.tensor([3, 2], dtype=torch.int32)
+    r = torch.tensor([1, 0], dtype=torch.int32)
+    k = torch.tensor([0, 1], dtype=torch.int8)
+    A = torch.zeros(13, dtype=torch.float64)
+    B = torch.zeros(3, dtype=torch.float64)
+    piv = torch.zeros(5, dtype=torch.int32)
+    info = torch.zeros(2, dtype=torch.int32)
+    with pytest.raises(ValueError):  # A one element short of 3*3 + 2*2
+        stream.solve_host(A[:12], B, piv, info, n, r, k)
+    with pytest.raises(ValueError):  # pivots short of 3 + 2
+        stream.solve_host(A, B, piv[:4], info, n, r, k)
+    with pytest.raises(ValueError):  # B missing while a matrix has a right-hand side
+        stream.solve_host(A, None, piv, info, n, r, k)
+    with pytest.raises(TypeError):
+        stream.solve_host(A, B.float(), piv, info, n, r, k)
+    with pytest.raises(TypeError):
+        stream.solve_host(A, B, piv, info, n.long(), r, k)
+    with pytest.raises(ValueError):
+        stream.solve_host(A, B, piv, info[:1], n, r, k)
+    e = torch.zeros(0, dtype=torch.int32)
+    stream.solve_host(A, B, piv, info, e, e, torch.zeros(0, dtype=torch.int8))  # count 0: nothing to do
