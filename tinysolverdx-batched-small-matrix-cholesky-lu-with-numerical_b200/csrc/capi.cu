@@ -186,31 +186,42 @@ int run_host(Kind kind, T* A, const int* piv_in, int n, int64_t batch, T* B, int
   const bool writes_a = (kind == POTRF || kind == GETRF || kind == POSV || kind == GESV) && !keep_a;
   const bool writes_piv = (kind == GETRF || kind == GESV) && !keep_a;
   const bool writes_info = info && (kind == POTRF || kind == GETRF || kind == POSV || kind == GESV);
-  int c = 0;
-  for (int64_t m = 0; m < batch; m += chunk, ++c) {
-    Slot& s = ctx.slot[c % kSlots];
-    const int64_t cnt = std::min(chunk, batch - m);
-    T* dA = static_cast<T*>(s.a);
-    T* dB = static_cast<T*>(s.b);
-    TSDX_CK(cudaMemcpyAsync(dA, reinterpret_cast<const char*>(A) + m * mat, mat * cnt, cudaMemcpyHostToDevice, s.st), "H2D A");
-    if (has_b && nrhs > 0)
-      TSDX_CK(cudaMemcpyAsync(dB, reinterpret_cast<const char*>(B) + m * rhs, rhs * cnt, cudaMemcpyHostToDevice, s.st), "H2D B");
-    if (kind == GETRS)
-      TSDX_CK(cudaMemcpyAsync(s.piv, piv_in + m * n, size_t(n) * cnt * sizeof(int), cudaMemcpyHostToDevice, s.st), "H2D piv");
-    // the device workspace copy of A may take the factor even when the caller's A is kept
-    const int rc = run_device<T>(kind, dA, s.piv, n, cnt, dB, nrhs, s.piv, writes_info ? s.info : nullptr, s.st);
-    if (rc) return rc;
-    if (writes_a)
-      TSDX_CK(cudaMemcpyAsync(reinterpret_cast<char*>(A) + m * mat, dA, mat * cnt, cudaMemcpyDeviceToHost, s.st), "D2H A");
-    if (has_b && nrhs > 0)
-      TSDX_CK(cudaMemcpyAsync(reinterpret_cast<char*>(B) + m * rhs, dB, rhs * cnt, cudaMemcpyDeviceToHost, s.st), "D2H B");
-    if (writes_piv)
-      TSDX_CK(cudaMemcpyAsync(piv + m * n, s.piv, size_t(n) * cnt * sizeof(int), cudaMemcpyDeviceToHost, s.st), "D2H piv");
-    if (writes_info)
-      TSDX_CK(cudaMemcpyAsync(info + m, s.info, size_t(cnt) * sizeof(int), cudaMemcpyDeviceToHost, s.st), "D2H info");
+  auto enqueue = [&]() -> int {
+    int c = 0;
+    for (int64_t m = 0; m < batch; m += chunk, ++c) {
+      Slot& s = ctx.slot[c % kSlots];
+      const int64_t cnt = std::min(chunk, batch - m);
+      T* dA = static_cast<T*>(s.a);
+      T* dB = static_cast<T*>(s.b);
+      TSDX_CK(cudaMemcpyAsync(dA, reinterpret_cast<const char*>(A) + m * mat, mat * cnt, cudaMemcpyHostToDevice, s.st), "H2D A");
+      if (has_b && nrhs > 0)
+        TSDX_CK(cudaMemcpyAsync(dB, reinterpret_cast<const char*>(B) + m * rhs, rhs * cnt, cudaMemcpyHostToDevice, s.st), "H2D B");
+      if (kind == GETRS)
+        TSDX_CK(cudaMemcpyAsync(s.piv, piv_in + m * n, size_t(n) * cnt * sizeof(int), cudaMemcpyHostToDevice, s.st), "H2D piv");
+      // the device workspace copy of A may take the factor even when the caller's A is kept
+      const int rc = run_device<T>(kind, dA, s.piv, n, cnt, dB, nrhs, s.piv, writes_info ? s.info : nullptr, s.st);
+      if (rc) return rc;
+      if (writes_a)
+        TSDX_CK(cudaMemcpyAsync(reinterpret_cast<char*>(A) + m * mat, dA, mat * cnt, cudaMemcpyDeviceToHost, s.st), "D2H A");
+      if (has_b && nrhs > 0)
+        TSDX_CK(cudaMemcpyAsync(reinterpret_cast<char*>(B) + m * rhs, dB, rhs * cnt, cudaMemcpyDeviceToHost, s.st), "D2H B");
+      if (writes_piv)
+        TSDX_CK(cudaMemcpyAsync(piv + m * n, s.piv, size_t(n) * cnt * sizeof(int), cudaMemcpyDeviceToHost, s.st), "D2H piv");
+      if (writes_info)
+        TSDX_CK(cudaMemcpyAsync(info + m, s.info, size_t(cnt) * sizeof(int), cudaMemcpyDeviceToHost, s.st), "D2H info");
+    }
+    return TSDX_OK;
+  };
+  // drain the slots' streams on failure too: no copy into the caller's buffers outlives the call
+  int rc = enqueue();
+  for (auto& s : ctx.slot) {
+    const cudaError_t e = cudaStreamSynchronize(s.st);
+    if (e != cudaSuccess && rc == TSDX_OK) {
+      set_cuda_error(e, "cudaStreamSynchronize");
+      rc = TSDX_ERR_CUDA;
+    }
   }
-  for (auto& s : ctx.slot) TSDX_CK(cudaStreamSynchronize(s.st), "cudaStreamSynchronize");
-  return TSDX_OK;
+  return rc;
 }
 
 }  // namespace

@@ -246,20 +246,23 @@ class Selector:
         streams = [torch.cuda.Stream(self.device) for _ in range(slots)]
         for st in streams:
             st.wait_stream(cur)  # the slot buffers were allocated on the current stream
-        for c, (A, b, spd, n, i0, i1, (info, status, tier)) in enumerate(jobs):
-            k, cnt = c % slots, i1 - i0
-            # slot k's buffers are reused by chunk c + slots on the same stream, after
-            # this chunk's copies back; the solve's own temporaries live on that stream too
-            with torch.cuda.stream(streams[k]):
-                dA = bufA[k][:cnt * n * n].view(cnt, n, n)
-                dx = bufx[k][:cnt * n].view(cnt, n)
-                dA.copy_(A[i0:i1], non_blocking=True)
-                dx.copy_(b[i0:i1], non_blocking=True)
-                inf, stt, _, tr = self.solve(dA, dx, spd, itmax=itmax, tol=tol)
-                b[i0:i1].copy_(dx, non_blocking=True)
-                info[i0:i1].copy_(inf, non_blocking=True)
-                status[i0:i1].copy_(stt, non_blocking=True)
-                tier[i0:i1].copy_(tr, non_blocking=True)
-        for st in streams:
-            st.synchronize()
+        try:
+            for c, (A, b, spd, n, i0, i1, (info, status, tier)) in enumerate(jobs):
+                k, cnt = c % slots, i1 - i0
+                # slot k's buffers are reused by chunk c + slots on the same stream, after
+                # this chunk's copies back; the solve's own temporaries live on that stream too
+                with torch.cuda.stream(streams[k]):
+                    dA = bufA[k][:cnt * n * n].view(cnt, n, n)
+                    dx = bufx[k][:cnt * n].view(cnt, n)
+                    dA.copy_(A[i0:i1], non_blocking=True)
+                    dx.copy_(b[i0:i1], non_blocking=True)
+                    inf, stt, _, tr = self.solve(dA, dx, spd, itmax=itmax, tol=tol)
+                    b[i0:i1].copy_(dx, non_blocking=True)
+                    info[i0:i1].copy_(inf, non_blocking=True)
+                    status[i0:i1].copy_(stt, non_blocking=True)
+                    tier[i0:i1].copy_(tr, non_blocking=True)
+        finally:
+            # also on an error: no copy into the caller's buffers outlives the call
+            for st in streams:
+                st.synchronize()
         return outs
