@@ -252,3 +252,18 @@ def test_stream_host_many_chunks_pinned(dtype):
     dP[:chol.numel()][chol] = -7
     check_host_equals_device(host, (dev_out[0], dev_out[1], dP, dev_out[3]), True)
     assert (host[3] == 0).mean(dtype=torch.float64) > 0.4  # the SPD half factors (info 0)
+
+
+def test_stream_host_no_rhs_no_info():
+    """Factor-only use of the host-memory call: every nrhs 0 (B NULL) and no info
+    buffer; factors and pivots match the device call."""
+    n, nrhs, kind, A, B = packed_random_stream(9, 3000, np.float64)
+    nrhs[:] = 0
+    _, _, _, na, nb, npv = stream.layout(torch.from_numpy(n), torch.from_numpy(nrhs))
+    assert nb == 0
+    hA = A.clone()
+    piv = torch.zeros(npv, dtype=torch.int32)
+    stream.solve_host(hA, None, piv, None, torch.from_numpy(n), torch.from_numpy(nrhs), torch.from_numpy(kind))
+    dA, _, dP, _ = run_direct(n, nrhs, kind, A, B[:1], True, 0)
+    assert bits_equal(hA, dA.cpu())
+    assert torch.equal(piv, dP.cpu())
