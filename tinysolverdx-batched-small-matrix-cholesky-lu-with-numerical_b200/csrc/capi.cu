@@ -345,14 +345,17 @@ int stream_entry(T* A, const int64_t* aoff, T* B, const int64_t* boff, int* piv,
 }
 
 // ---- uneven stream from host memory ------------------------------------------------
-// The packed set is cut into chunks of about kStreamChunkBytes of A, in index order. A
-// chunk travels with its own metadata record (offsets rebased to the chunk's first
-// matrix, orders, right-hand-side counts, kinds), so the device holds kStreamSlots
-// chunks at a time whatever the size of the set, and chunk c's host->device copy,
-// chunk c-1's sort and drain and chunk c-2's device->host copy run at the same time on
-// the slots' streams. One host pass validates every entry and cuts the chunks before
-// anything is copied; each chunk's record is written just before its copies are
-// queued, while the earlier chunks are in flight.
+// The packed set is cut into chunks of about kStreamChunkBytes, in index order, counting
+// every byte a matrix moves or occupies (A, B, pivots, info, its metadata record and
+// sort scratch). A chunk travels with its own metadata record (offsets rebased to the
+// chunk's first matrix, orders, right-hand-side counts, kinds), so the device holds
+// kStreamSlots chunks at a time whatever the size of the set, and chunk c's host->device
+// copy, chunk c-1's sort and drain and chunk c-2's device->host copy run at the same time
+// on the slots' streams. One host pass validates every entry and cuts the chunks before
+// anything is copied. Each slot has one pinned record buffer: chunk c's record is
+// written into it once chunk c - kStreamSlots's record upload has finished (an event),
+// just before chunk c's copies are queued, so pinned memory is bounded by the chunk
+// size too.
 constexpr int kStreamSlots = 3;
 constexpr size_t kStreamChunkBytes = size_t(96) << 20;
 
@@ -368,13 +371,16 @@ struct StreamSlotWs {
 struct StreamHostCtx {
   StreamSlotWs ws[kStreamSlots];
   bool init = false;
-  void* hmeta = nullptr;  // pinned: every chunk's metadata record of the current call
+  void* hrec[kStreamSlots] = {};            // pinned record buffer of each slot
+  cudaEvent_t rec_sent[kStreamSlots] = {};  // the slot's last record upload has finished
   size_t hcap = 0;
 };
 StreamHostCtx g_stream_ctx[64];
 
 // record of cnt matrices: aoff, boff, poff (int64), n, nrhs (int32), kind (int8)
 constexpr size_t meta_record_bytes(int64_t cnt) { return (size_t(cnt) * 33 + 255) / 256 * 256; }
+// host and device bytes of one matrix beyond its A, B and pivots: record, info, sort scratch
+constexpr size_t kStreamPerMatrixBytes = 33 + 4 + 4;
 
 template <class T>
 int stream_host_entry(T* A, T* B, int* piv, int* info, const int* n, const int* nrhs, const signed char* kind,
@@ -391,10 +397,11 @@ int stream_host_entry(T* A, T* B, int* piv, int* info, const int* n, const int* 
   };
   std::vector<int64_t> first;
   std::vector<Ext> ext;
-  int64_t mx_cnt = 0, mx_a = 0, mx_b = 0, mx_p = 0, meta_total = 0;
+  int64_t mx_cnt = 0, mx_a = 0, mx_b = 0, mx_p = 0;
   bool any_b = false;
   {
     int64_t i0 = 0, a = 0, b = 0, p = 0;
+    size_t bytes = 0;
     for (int64_t i = 0; i < count; ++i) {
       const int ni = n[i], ri = nrhs[i];
       if (ni < 1 || ni > 64) return TSDX_ERR_N;
@@ -402,7 +409,8 @@ int stream_host_entry(T* A, T* B, int* piv, int* info, const int* n, const int* 
       a += int64_t(ni) * ni;
       b += int64_t(ni) * ri;
       p += ni;
-      if (size_t(a) * sizeof(T) >= kStreamChunkBytes || i + 1 == count) {
+      bytes += size_t(ni) * (ni + ri) * sizeof(T) + size_t(ni) * sizeof(int) + kStreamPerMatrixBytes;
+      if (bytes >= kStreamChunkBytes || i + 1 == count) {
         first.push_back(i0);
         ext.push_back({a, b, p});
         mx_cnt = std::max(mx_cnt, i + 1 - i0);
@@ -410,9 +418,9 @@ int stream_host_entry(T* A, T* B, int* piv, int* info, const int* n, const int* 
         mx_b = std::max(mx_b, b);
         mx_p = std::max(mx_p, p);
         any_b = any_b || b > 0;
-        meta_total += int64_t(meta_record_bytes(i + 1 - i0));
         i0 = i + 1;
         a = b = p = 0;
+        bytes = 0;
       }
     }
     first.push_back(count);
@@ -426,6 +434,7 @@ int stream_host_entry(T* A, T* B, int* piv, int* info, const int* n, const int* 
   StreamHostCtx& sc = g_stream_ctx[devi];
   if (!sc.init) {
     for (auto& w : sc.ws) TSDX_CK(cudaStreamCreateWithFlags(&w.st, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (auto& e : sc.rec_sent) TSDX_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
     sc.init = true;
   }
   const size_t scratch_bytes = size_t(tsdx::host::stream_scratch_bytes(mx_cnt));
@@ -440,23 +449,27 @@ int stream_host_entry(T* A, T* B, int* piv, int* info, const int* n, const int* 
       if (int rc = grow(reinterpret_cast<void**>(&w.info), &w.icap, size_t(mx_cnt) * sizeof(int))) return rc;
     if (int rc = grow(&w.meta, &w.mcap, meta_record_bytes(mx_cnt) + scratch_bytes)) return rc;
   }
-  if (size_t(meta_total) > sc.hcap) {
-    // the previous call synchronized its streams before returning: nothing reads the old buffer
-    if (sc.hmeta) cudaFreeHost(sc.hmeta);
-    sc.hmeta = nullptr;
+  if (meta_record_bytes(mx_cnt) > sc.hcap) {
+    // the previous call synchronized its streams before returning: nothing reads the old buffers
+    for (auto& h : sc.hrec) {
+      if (h) cudaFreeHost(h);
+      h = nullptr;
+    }
     sc.hcap = 0;
-    TSDX_CK(cudaMallocHost(&sc.hmeta, size_t(meta_total)), "cudaMallocHost");
-    sc.hcap = size_t(meta_total);
+    for (auto& h : sc.hrec) TSDX_CK(cudaMallocHost(&h, meta_record_bytes(mx_cnt)), "cudaMallocHost");
+    sc.hcap = meta_record_bytes(mx_cnt);
   }
 
   const int nchunks = int(first.size()) - 1;
   auto enqueue = [&]() -> int {
-    unsigned char* rec = static_cast<unsigned char*>(sc.hmeta);
     int64_t a0 = 0, b0 = 0, p0 = 0;
     for (int c = 0; c < nchunks; ++c) {
       const int64_t i0 = first[c], cnt = first[c + 1] - i0;
       const int64_t ca = ext[c].a, cb = ext[c].b, cp = ext[c].p;
-      // this chunk's record, in its own region of the pinned buffer
+      const int k = c % kStreamSlots;
+      unsigned char* rec = static_cast<unsigned char*>(sc.hrec[k]);
+      // this chunk's record, once the slot's previous record has reached the device
+      if (c >= kStreamSlots) TSDX_CK(cudaEventSynchronize(sc.rec_sent[k]), "cudaEventSynchronize");
       {
         int64_t* ao = reinterpret_cast<int64_t*>(rec);
         int64_t* bo = ao + cnt;
@@ -478,11 +491,12 @@ int stream_host_entry(T* A, T* B, int* piv, int* info, const int* n, const int* 
           p += ni;
         }
       }
-      const StreamSlotWs& w = sc.ws[c % kStreamSlots];
+      const StreamSlotWs& w = sc.ws[k];
       const cudaStream_t st = w.st;
       const size_t rb = meta_record_bytes(cnt);
       unsigned char* dm = static_cast<unsigned char*>(w.meta);
       TSDX_CK(cudaMemcpyAsync(dm, rec, size_t(cnt) * 33, cudaMemcpyHostToDevice, st), "H2D stream record");
+      TSDX_CK(cudaEventRecord(sc.rec_sent[k], st), "cudaEventRecord");
       TSDX_CK(cudaMemcpyAsync(w.a, A + a0, size_t(ca) * sizeof(T), cudaMemcpyHostToDevice, st), "H2D A");
       if (cb > 0) TSDX_CK(cudaMemcpyAsync(w.b, B + b0, size_t(cb) * sizeof(T), cudaMemcpyHostToDevice, st), "H2D B");
       // the solve writes no pivots for Cholesky matrices: their slots go in and come
@@ -511,7 +525,6 @@ int stream_host_entry(T* A, T* B, int* piv, int* info, const int* n, const int* 
       if (cb > 0) TSDX_CK(cudaMemcpyAsync(B + b0, w.b, size_t(cb) * sizeof(T), cudaMemcpyDeviceToHost, st), "D2H B");
       if (info)
         TSDX_CK(cudaMemcpyAsync(info + i0, w.info, size_t(cnt) * sizeof(int), cudaMemcpyDeviceToHost, st), "D2H info");
-      rec += rb;
       a0 += ca;
       b0 += cb;
       p0 += cp;
