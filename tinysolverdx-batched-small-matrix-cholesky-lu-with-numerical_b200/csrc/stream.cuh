@@ -14,12 +14,14 @@
 // bucket = (kind, padded order NP in {8, 16, ..., 64}, right-hand-side class
 // {<= 2, <= 8}); each bucket is cut into work units of S matrices (S = 32/G
 // segments per warp for NP <= 32, as unit_size lists; or one warp per matrix when
-// the tuned schedule asks for it). One persistent launch then drains the units through a global
-// atomic queue, largest order first, so at any moment the SMs run mostly the same
-// code variant and the smallest units fill the tail; each unit is the same
-// per-matrix body (blk.cuh) as the dense kernels, so the results are
-// bit-identical to them. The four launches are capturable in a CUDA graph (no
-// host synchronisation; scratch passed in by the caller).
+// the tuned schedule asks for it). Three persistent launches then drain the units
+// through global atomic queues, one per group of order classes (n 57..64, n 49..56,
+// n <= 48), largest orders first: each group's warps get the shared memory of its own
+// largest variant, so the smaller orders keep more warps per SM, and within a group the
+// SMs run mostly the same code variant with the smallest units filling the tail. Each
+// unit is the same per-matrix body (blk.cuh) as the dense kernels, so the results are
+// bit-identical to them. The launches are capturable in a CUDA graph (no host
+// synchronisation; scratch passed in by the caller).
 #pragma once
 #include "blk.cuh"
 
@@ -157,29 +159,35 @@ __device__ __forceinline__ void stream_unit(unsigned char* M, const StreamArgs<T
   blk_matrix<T, NP, NRHS, CHOL, G>(M + (lane / G) * BlkCfg<T, NP, NRHS, G>::SEGB, j, g);
 }
 
-// Persistent drain of the bucket-ordered work units. Every warp owns WARPB bytes
-// of shared memory, sized for the largest variant.
-template <class T, int WARPB, int WPC>
+// Persistent drain of the work units of order classes CLO..CHI (one launch per class
+// group, largest orders first). Every warp owns WARPB bytes of shared memory, sized for
+// the largest variant of its group, so the groups of smaller orders keep more warps per
+// SM. The classes' buckets are contiguous in bucket order, hence so are their units.
+// The group's queue head is the bucket cursor cur[CLO]: the cursors are dead once the
+// scatter has run, and the host zeroes them before the drains.
+template <class T, int WARPB, int WPC, int CLO, int CHI>
 __global__ void __launch_bounds__(WPC * 32, 1) stream_kernel(StreamArgs<T> a) {
+  static_assert(0 <= CLO && CLO <= CHI && CHI < kStreamClasses, "class range");
+  constexpr int B_LO = (kStreamClasses - 1 - CHI) * 4, B_HI = (kStreamClasses - CLO) * 4;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ int ustart_s[kStreamBuckets + 1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int* start = a.scratch + kStreamBuckets;
   const int* cnt = a.scratch;
   const int* ustart = a.scratch + 3 * kStreamBuckets;
-  int* head = a.scratch + 4 * kStreamBuckets + 1;
+  int* head = a.scratch + 2 * kStreamBuckets + CLO;
   const int* perm = a.scratch + 4 * kStreamBuckets + 2;
   if (threadIdx.x <= kStreamBuckets) ustart_s[threadIdx.x] = ustart[threadIdx.x];
   __syncthreads();
-  const int total = ustart_s[kStreamBuckets];
+  const int u0 = ustart_s[B_LO], total = ustart_s[B_HI];
   unsigned char* M = smem + warp * WARPB;
   for (;;) {
     int w = 0;
-    if (lane == 0) w = atomicAdd(head, 1);
+    if (lane == 0) w = u0 + atomicAdd(head, 1);
     w = __shfl_sync(kFull, w, 0);
     if (w >= total) break;
-    int b = 0;
-    while (b + 1 < kStreamBuckets && ustart_s[b + 1] <= w) ++b;
+    int b = B_LO;
+    while (b + 1 < B_HI && ustart_s[b + 1] <= w) ++b;
     const int us = unit_size<T>(b, a.sched);
     const int first = start[b] + (w - ustart_s[b]) * us;
     const int last = min(first + us, start[b] + cnt[b]);
@@ -195,7 +203,8 @@ __global__ void __launch_bounds__(WPC * 32, 1) stream_kernel(StreamArgs<T> a) {
   else { TSDX_SU_KIND(NP_, 2, G_); }
     switch (c) {
       case 0:
-        if (one) {
+        if constexpr (CLO > 0) {
+        } else if (one) {
           TSDX_SU_RHS(8, 32)
         } else if (wide) {
           if (lu) TSDX_SU(8, 8, false, 8);
@@ -205,9 +214,14 @@ __global__ void __launch_bounds__(WPC * 32, 1) stream_kernel(StreamArgs<T> a) {
           else TSDX_SU(8, 2, true, 4);
         }
         break;
-      case 1: if (one) { TSDX_SU_RHS(16, 32) } else { TSDX_SU_RHS(16, 8) } break;
+      case 1:
+        if constexpr (CLO <= 1 && CHI >= 1) {
+          if (one) { TSDX_SU_RHS(16, 32) } else { TSDX_SU_RHS(16, 8) }
+        }
+        break;
       case 2:
-        if (one) {
+        if constexpr (CLO > 2 || CHI < 2) {
+        } else if (one) {
           TSDX_SU_RHS(24, 32)
         } else if constexpr (sizeof(T) == 4) {
           TSDX_SU_RHS(24, 8)
@@ -215,11 +229,23 @@ __global__ void __launch_bounds__(WPC * 32, 1) stream_kernel(StreamArgs<T> a) {
           TSDX_SU_RHS(24, 16)
         }
         break;
-      case 3: if (one) { TSDX_SU_RHS(32, 32) } else { TSDX_SU_RHS(32, 16) } break;
-      case 4: TSDX_SU_RHS(40, 32) break;
-      case 5: TSDX_SU_RHS(48, 32) break;
-      case 6: TSDX_SU_RHS(56, 32) break;
-      default: TSDX_SU_RHS(64, 32) break;
+      case 3:
+        if constexpr (CLO <= 3 && CHI >= 3) {
+          if (one) { TSDX_SU_RHS(32, 32) } else { TSDX_SU_RHS(32, 16) }
+        }
+        break;
+      case 4:
+        if constexpr (CLO <= 4 && CHI >= 4) { TSDX_SU_RHS(40, 32) }
+        break;
+      case 5:
+        if constexpr (CLO <= 5 && CHI >= 5) { TSDX_SU_RHS(48, 32) }
+        break;
+      case 6:
+        if constexpr (CLO <= 6 && CHI >= 6) { TSDX_SU_RHS(56, 32) }
+        break;
+      default:
+        if constexpr (CHI >= 7) { TSDX_SU_RHS(64, 32) }
+        break;
     }
 #undef TSDX_SU_RHS
 #undef TSDX_SU_KIND

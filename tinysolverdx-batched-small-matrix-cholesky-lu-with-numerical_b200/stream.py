@@ -11,7 +11,7 @@ TinySolverDx itself has no such call (its batched entry points take one
 module is the mixed-workload path on top of the same per-matrix solvers.
 
 ``StreamPlan`` fixes a layout once, picks the fastest warp schedule for it by timing
-the candidates on the device (the autotuner), captures the four launches of a solve
+the candidates on the device (the autotuner), captures the launches of a solve
 in a CUDA graph and replays it on new data.
 """
 import torch
@@ -193,7 +193,7 @@ class StreamPlan:
         return self.sched
 
     def capture(self):
-        """Capture one solve (memset + histogram + scan + scatter + drain) in a CUDA graph."""
+        """Capture one solve (memset, histogram, scan, scatter, memset, three drains) in a CUDA graph."""
         s = torch.cuda.Stream(self.device)
         s.wait_stream(torch.cuda.current_stream(self.device))
         with torch.cuda.stream(s):
