@@ -515,6 +515,15 @@ def _emit(a, world, value, ms, dt, cfg, roof, cpu, e2e, clk, launches, extra=Non
     print(json.dumps(out), flush=True)
 
 
+def link_ceiling_ms(h2d_bytes, d2h_bytes, up_gbs, down_gbs, both_gbs):
+    """Least time (ms) to move h2d_bytes in and d2h_bytes out with the two directions
+    overlapped: the smaller byte count at the two-way rate (GB/s per direction), the
+    rest of the larger direction at its one-way rate."""
+    h, d = float(h2d_bytes), float(d2h_bytes)
+    rest = (h - d) / up_gbs if h >= d else (d - h) / down_gbs
+    return (min(h, d) / both_gbs + rest) / 1e6
+
+
 def _link(e2e):
     """Attach the host link's ceiling to an e2e record. Pinned host<->device copies
     of 1 GiB are timed host->device alone, device->host alone and both ways at once.
@@ -556,8 +565,7 @@ def _link(e2e):
 
     r_up, r_down, r_both = rate(True, False), rate(False, True), rate(True, True)
     h, d = e2e["h2d_bytes_per_step"], e2e["d2h_bytes_per_step"]
-    ceil_s = min(h, d) / (r_both * 1e9) + (h - d) / (r_up * 1e9) if h >= d else \
-        min(h, d) / (r_both * 1e9) + (d - h) / (r_down * 1e9)
+    ceil_s = link_ceiling_ms(h, d, r_up, r_down, r_both) * 1e-3
     ach = max(h, d) / (e2e["ms_per_step"] * 1e-3) / 1e9
     e2e["link"] = {"bound": "pcie", "achieved": round(ach, 1), "unit": "GB/s (larger direction)",
                    "h2d_alone": round(r_up, 1), "d2h_alone": round(r_down, 1), "both_ways": round(r_both, 1),

@@ -1,0 +1,26 @@
+"""Host-side arithmetic of bench.py (no GPU): the e2e link-ceiling model."""
+import importlib.util
+
+import pytest
+
+from conftest import ROOT
+
+
+def _bench():
+    spec = importlib.util.spec_from_file_location("bench_mod", ROOT / "bench.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_link_ceiling_model():
+    f = _bench().link_ceiling_ms
+    # equal traffic both ways: all of it at the two-way rate
+    assert f(44.3e9, 44.3e9, 55.0, 52.0, 44.3) == pytest.approx(1000.0)
+    # one way only: the one-way rate
+    assert f(55.6e9, 0, 55.6, 52.0, 44.3) == pytest.approx(1000.0)
+    assert f(0, 52.0e9, 55.6, 52.0, 44.3) == pytest.approx(1000.0)
+    # mixed: 1 GB both ways at 40 GB/s (25 ms), the other 2 GB in at 60 GB/s (33.3 ms)
+    assert f(3e9, 1e9, 60.0, 50.0, 40.0) == pytest.approx(25.0 + 2e9 / 60e6)
+    # mixed, larger outbound: 1 GB both ways (25 ms), 1 GB more out at 50 GB/s (20 ms)
+    assert f(1e9, 2e9, 60.0, 50.0, 40.0) == pytest.approx(45.0)
