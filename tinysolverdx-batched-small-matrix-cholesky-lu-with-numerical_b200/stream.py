@@ -102,7 +102,7 @@ def solve_host(A, B, piv, info, n, nrhs, kind, write_factors=True, sched=0):
 
     Same arguments as ``solve`` without the offsets, all CPU tensors: the matrices
     are packed back to back in index order (``layout``'s offsets). The library moves
-    the set through the device in chunks of about 96 MB of A with the copies of one
+    the set through the device in chunks of about 96 MB with the copies of one
     chunk overlapping the solve of the next, so the device never holds the whole set.
     Pin A, B, piv and info (``tensor.pin_memory()``) for the copies to overlap.
     Raises on n outside [1, 64] or nrhs outside [0, 8] before anything is copied.
