@@ -195,11 +195,10 @@ int tsdx_cuda_solve_stream_f64(double* A, const int64_t* aoff, double* B, const 
  * order: matrix i's A at sum_{j<i} n_j^2 elements, its right-hand sides at
  * sum_{j<i} n_j*nrhs_j, its pivots at sum_{j<i} n_j (the packing of the Python
  * layer's stream.layout). n, nrhs and kind are host arrays too. Synchronous, like the
- * *_batched_host_* calls: the set crosses the device in chunks of about 96 MB (every byte
- * a matrix moves counted), so
- * the device holds three chunks at a time whatever the size of the set, and each
- * chunk's host->device copy overlaps the previous chunk's solve and the device->host
- * copy of the one before. The copies overlap only when the host buffers are pinned
+ * *_batched_host_* calls: the set crosses the device in chunks of about 96 MB (every
+ * byte a matrix moves counted), so the device holds three chunks at a time whatever
+ * the size of the set, and each chunk's host->device copy overlaps the previous
+ * chunk's solve and the device->host copy of the one before. The copies overlap only when the host buffers are pinned
  * (page-locked); pageable buffers work but serialize. Every entry is checked before
  * any copy: n outside [1, 64] -> TSDX_ERR_N, nrhs outside [0, 8] -> TSDX_ERR_NRHS.
  * B may be NULL when every nrhs is 0, piv when write_factors is 0; info may be NULL.
