@@ -24,3 +24,23 @@ def test_link_ceiling_model():
     assert f(3e9, 1e9, 60.0, 50.0, 40.0) == pytest.approx(25.0 + 2e9 / 60e6)
     # mixed, larger outbound: 1 GB both ways (25 ms), 1 GB more out at 50 GB/s (20 ms)
     assert f(1e9, 2e9, 60.0, 50.0, 40.0) == pytest.approx(45.0)
+
+
+def test_reference_arm_contract():
+    """bench.py --impl reference runs the reference library (compiled from its sources
+    into oracle/_ref) on the host and prints one JSON line with the fields the
+    comparison needs; it needs no GPU."""
+    import json
+    import subprocess
+    import sys
+    if not (ROOT / "oracle" / "_ref" / "libtsdx_ref.so").exists():
+        pytest.skip("oracle/_ref not built")
+    out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--workload", "posv_f64_n16",
+                          "--steps", "1", "--warmup", "3"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    d = json.loads(out.stdout.strip().splitlines()[-1])
+    assert d["impl"] == "reference" and d["unit"] == "solves/s" and d["value"] > 0
+    assert d["higher_is_better"] is True and d["n_gpus"] == 1 and d["steps"] == 1 and d["warmup"] >= 3
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["value"] == d["value"] and cb["cores"] >= 1 and cb["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
