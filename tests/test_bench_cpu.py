@@ -44,3 +44,26 @@ def test_reference_arm_contract():
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["value"] == d["value"] and cb["cores"] >= 1 and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_reference_arm_under_torchrun_two_ranks():
+    """Launched like the multi-GPU runs (torchrun, 2 ranks): rank 0 alone runs the
+    reference and prints one line; the other rank exits 0 without work."""
+    import json
+    import socket
+    import subprocess
+    import sys
+    if not (ROOT / "oracle" / "_ref" / "libtsdx_ref.so").exists():
+        pytest.skip("oracle/_ref not built")
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
+           "127.0.0.1", "--master-port", str(port), str(ROOT / "bench.py"), "--impl", "reference", "--gpus", "2",
+           "--workload", "posv_f64_n16", "--steps", "1", "--warmup", "3"]
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.strip().splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["value"] > 0
