@@ -184,13 +184,14 @@ def posv_ir(A, b, tier="fp32", itmax=3, tol=1e-15):
 
 
 def solve_stream(mats, rhs, kinds, write_factors=False):
-    """Solve a ragged list of systems in one GPU call (the uneven stream).
+    """Solve a ragged list of systems with the uneven-stream kernels in one call.
 
     mats: sequence of (n_i, n_i) float32 or float64 arrays (one dtype for all), n_i in 1..64;
     rhs: sequence of (n_i,) or (n_i, k_i) arrays, k_i in 0..8 (None -> no right-hand side);
     kinds: sequence of "cholesky"/"lu" (or 0/1). Returns (X list, info array), plus
     (factors list, pivots list) when write_factors. Factors, pivots, info and X are
-    bit-identical to ``posv``/``gesv`` with backend="cuda" on each matrix.
+    bit-identical to ``posv``/``gesv`` with backend="cuda" on each matrix. The set moves
+    through the device in chunks of about 96 MB, so it may exceed device memory.
     """
     import torch
     from . import stream as _stream
@@ -221,23 +222,24 @@ def solve_stream(mats, rhs, kinds, write_factors=False):
         bs.append(b)
     nrhs = np.array([b.shape[1] for b in bs], np.int32)
     aoff, boff, poff, *_ = _stream.layout(ns, nrhs)
-    dev = torch.device("cuda")
-    A = torch.from_numpy(np.concatenate([np.ascontiguousarray(a).ravel() for a in mats])).to(dev)
+    # the host-memory stream call moves the set through the device in chunks, so the set
+    # may be larger than device memory
+    A = torch.from_numpy(np.concatenate([np.ascontiguousarray(a).ravel() for a in mats]))
     Bh = np.concatenate([b.ravel() for b in bs])
-    B = torch.from_numpy(Bh if Bh.size else np.zeros(1, dt)).to(dev)
-    piv = torch.zeros(int(ns.sum()), dtype=torch.int32, device=dev)
-    info = torch.zeros(count, dtype=torch.int32, device=dev)
-    t = lambda x, d: torch.from_numpy(np.ascontiguousarray(x, d)).to(dev)  # noqa: E731
-    _stream.solve(A, t(aoff.numpy(), np.int64), B, t(boff.numpy(), np.int64), piv, t(poff.numpy(), np.int64), info,
-                  t(ns, np.int32), t(nrhs, np.int32), t(kind, np.int8), write_factors=write_factors)
-    Xh, infoh = B.cpu().numpy(), info.cpu().numpy()
+    B = torch.from_numpy(Bh if Bh.size else np.zeros(1, dt))
+    piv = torch.zeros(int(ns.sum()), dtype=torch.int32)
+    info = torch.zeros(count, dtype=torch.int32)
+    _stream.solve_host(A, B, piv, info, torch.from_numpy(np.ascontiguousarray(ns, np.int32)),
+                       torch.from_numpy(np.ascontiguousarray(nrhs, np.int32)),
+                       torch.from_numpy(np.ascontiguousarray(kind, np.int8)), write_factors=write_factors)
+    Xh, infoh = B.numpy(), info.numpy()
     X = []
     for i, (n, k) in enumerate(zip(ns, nrhs)):
         x = Xh[boff[i]:boff[i] + n * k].reshape(n, k)
         X.append(x[:, 0].copy() if vec[i] else x.copy())
     if not write_factors:
         return X, infoh
-    Ah, ph = A.cpu().numpy(), piv.cpu().numpy()
+    Ah, ph = A.numpy(), piv.numpy()
     F = [Ah[aoff[i]:aoff[i] + n * n].reshape(n, n).copy() for i, n in enumerate(ns)]
     P = [ph[poff[i]:poff[i] + n].copy() if kind[i] else None for i, n in enumerate(ns)]
     return X, infoh, F, P
