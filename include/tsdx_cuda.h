@@ -76,6 +76,11 @@ int tsdx_cuda_gesv_f64(double* A, int n, int64_t batch, double* B, int nrhs, int
  * solve and one-shot forms extend Backend::Cuda to the solves, which the
  * reference always runs on the CPU (batched.hpp:249, :260). Large batches are
  * streamed through the device in chunks so that the copies overlap the kernels.
+ * Memory kept after the call: the first call on a device creates three streams and
+ * three device slots sized for its chunk (at most 96 MB of A each, plus B, pivots and
+ * info); later calls reuse them and grow them when a chunk needs more. They are kept
+ * until the process exits (the uneven-stream host call below keeps its own three
+ * slots and pinned record buffers the same way).
  */
 int tsdx_cuda_cholesky_batched_host_f32(float* A, int n, int64_t batch, int* info);
 int tsdx_cuda_cholesky_batched_host_f64(double* A, int n, int64_t batch, int* info);
@@ -217,7 +222,9 @@ int tsdx_cuda_solve_stream_host_f64(double* A, double* B, int* piv, int* info, c
  * that loads the library keeps the array until exit. At most 262,144
  * matrices per call; a larger count returns TSDX_ERR_TOO_LARGE before any launch.
  * The array's address is looked up once per device on the first call on that device,
- * which must not be made while the stream is being captured. The bucket counters
+ * which must not be made while the stream is being captured, and is kept for the life
+ * of the process: it does not survive cudaDeviceReset, so do not call this entry point
+ * on a device again after resetting it. The bucket counters
  * that must start at zero are zeroed by every call on its stream. All calls on a
  * device share the array: calls whose executions overlap (other streams or threads)
  * race and corrupt each other's results, so order them (e.g. one stream). */

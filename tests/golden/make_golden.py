@@ -2,8 +2,8 @@
 
 Run where the reference tree is present (it reads it; nothing else does):
 
-    make -C oracle            # builds oracle/_ref/libtsdx_ref.so from the reference sources
-    python tests/golden/make_golden.py [/path/to/reference]
+    make -C oracle ref REF=/path/to/reference   # oracle/_ref/libtsdx_ref.so from its sources
+    python tests/golden/make_golden.py /path/to/reference   (or TSDX_REFERENCE=/path/to/reference)
 
 Inputs come from the reference's own generator (python/tinysolverdx/matrices.py,
 imported by path) and the reference tests' fixtures (tests/cpp/test_solvers.cpp
@@ -31,7 +31,7 @@ def ref_matrices(ref_root):
     return m
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root):
     M = ref_matrices(ref_root)
     R = Oracle("reference")
     out = {}
@@ -96,4 +96,8 @@ def main(ref_root="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    import os
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TSDX_REFERENCE")
+    if not root:
+        sys.exit("usage: make_golden.py <reference source tree>  (or set TSDX_REFERENCE)")
+    main(root)

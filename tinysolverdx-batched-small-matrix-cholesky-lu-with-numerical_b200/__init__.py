@@ -27,93 +27,108 @@ __all__ = ["cholesky", "lu", "cholesky_solve", "lu_solve", "posv", "gesv", "roun
            "chol_backward_error", "lu_backward_error", "solve_backward_error",
            "solve_forward_error", "reference_solve", "gesv_ir", "posv_ir", "solve_stream"]
 
-_DEFAULT_PREC = {np.dtype(np.float32): "fp32", np.dtype(np.float64): "fp64", np.dtype(np.float16): "fp16"}
+# The reference's Python layer (python/tinysolverdx/__init__.py:22-111), restated:
+#   storage dtype -> implied precision: float32 fp32, float64 fp64, float16 fp16,
+#     anything else TypeError (when no precision is given);
+#   precision must be fp16, bf16, fp32 or fp64 (ValueError otherwise);
+#   working dtype: float64 storage stays float64 whatever the precision (the core
+#     rounds into the target format), any other storage is handled as float32;
+#   float16 storage at precision fp16 comes back as float16;
+#   a single (n, n) matrix (and its (n,) or (n, k) right-hand side) is a batch of one.
+_IMPLIED_PRECISION = {np.dtype(np.float32): "fp32", np.dtype(np.float64): "fp64", np.dtype(np.float16): "fp16"}
+_PRECISIONS = ("fp16", "bf16", "fp32", "fp64")
+_NATIVE = {np.dtype(np.float32): "fp32", np.dtype(np.float64): "fp64"}
 
 
-def _fn(name, arr):
-    # one core entry point per storage dtype (no implicit casting)
-    return getattr(_core, f"{name}_{'f64' if arr.dtype == np.float64 else 'f32'}")
+class _Operand:
+    """A matrix argument normalised by the rules above."""
 
+    __slots__ = ("work", "precision", "single", "storage")
 
-def _prep(a, precision, ndim_single):
-    a = np.asarray(a)
-    single = a.ndim == ndim_single
-    if single:
-        a = a[None]
-    out_dtype = a.dtype
-    if precision is None:
-        if a.dtype not in _DEFAULT_PREC:
-            raise TypeError(f"unsupported dtype {a.dtype}; use float16/32/64")
-        precision = _DEFAULT_PREC[a.dtype]
-    if precision not in ("fp16", "bf16", "fp32", "fp64"):
-        raise ValueError("precision must be one of fp16, bf16, fp32, fp64")
-    work = np.float64 if (precision == "fp64" and a.dtype == np.float64) else np.float32
-    if a.dtype == np.float64 and precision != "fp64":
-        work = np.float64  # keep wide storage; the core rounds into the target format
-    return np.ascontiguousarray(a, dtype=work), precision, single, out_dtype
+    def __init__(self, a, precision):
+        a = np.asarray(a)
+        if precision is None:
+            precision = _IMPLIED_PRECISION.get(a.dtype)
+            if precision is None:
+                raise TypeError(f"unsupported dtype {a.dtype}; use float16/32/64")
+        elif precision not in _PRECISIONS:
+            raise ValueError("precision must be one of fp16, bf16, fp32, fp64")
+        self.precision = precision
+        self.storage = a.dtype
+        self.single = a.ndim == 2
+        wide = a.dtype == np.float64
+        self.work = np.ascontiguousarray(a[None] if self.single else a, dtype=np.float64 if wide else np.float32)
 
+    def entry(self, op):
+        """The core entry point of ``op`` for the working dtype."""
+        return getattr(_core, op + ("_f64" if self.work.dtype == np.float64 else "_f32"))
 
-def _finish(x, out_dtype, precision):
-    if precision == "fp16" and out_dtype == np.float16:
-        return x.astype(np.float16)
-    return x
+    def native(self):
+        """True when the precision is the working dtype's own (no emulation)."""
+        return _NATIVE.get(self.work.dtype) == self.precision
+
+    def cast(self, x):
+        return x.astype(np.float16) if (self.precision == "fp16" and self.storage == np.float16) else x
+
+    def unbatch(self, *results):
+        return tuple(r[0] for r in results) if self.single else results
+
+    def rhs(self, B):
+        """Right-hand sides stacked as (batch, n, k) in the working dtype, and whether
+        the caller passed one vector per matrix."""
+        B = np.asarray(B)
+        vector = B.ndim == (1 if self.single else 2)
+        if vector:
+            B = B[..., None]
+        if self.single:
+            B = B[None]
+        return np.ascontiguousarray(B, dtype=self.work.dtype), vector
+
+    def solution(self, X, vector):
+        X = X[..., 0] if vector else X
+        return X[0] if self.single else X
 
 
 def cholesky(A, precision=None, backend="auto"):
     """Lower Cholesky factors and LAPACK-style info (0 = ok, k>0: pivot k not positive)."""
-    a, p, single, dt = _prep(A, precision, 2)
-    L, info = _fn("cholesky", a)(a, p, backend)
-    L = _finish(L, dt, p)
-    return (L[0], info[0]) if single else (L, info)
+    op = _Operand(A, precision)
+    L, info = op.entry("cholesky")(op.work, op.precision, backend)
+    return op.unbatch(op.cast(L), info)
 
 
 def lu(A, precision=None, backend="auto"):
     """Packed LU with partial pivoting: (LU, piv, info). piv is scipy/LAPACK style (0-based)."""
-    a, p, single, dt = _prep(A, precision, 2)
-    LU, piv, info = _fn("lu", a)(a, p, backend)
-    LU = _finish(LU, dt, p)
-    return (LU[0], piv[0], info[0]) if single else (LU, piv, info)
-
-
-def _rhs(B, ref, single):
-    B = np.asarray(B)
-    if single:
-        B = B[:, None] if B.ndim == 1 else B
-        B = B[None]
-    elif B.ndim == 2:
-        B = B[:, :, None]
-    return np.ascontiguousarray(B, dtype=ref.dtype)
+    op = _Operand(A, precision)
+    LU, piv, info = op.entry("lu")(op.work, op.precision, backend)
+    return op.unbatch(op.cast(LU), piv, info)
 
 
 def cholesky_solve(L, B, precision=None, backend="auto"):
     """Solve L L^T x = B given factors from :func:`cholesky`."""
-    l, p, single, dt = _prep(np.asarray(L), precision, 2)
-    vec = np.asarray(B).ndim == (1 if single else 2)
-    X = _fn("cholesky_solve", l)(l, _rhs(B, l, single), p, backend)
-    X = _finish(X, dt, p)
-    X = X[..., 0] if vec else X
-    return X[0] if single else X
+    op = _Operand(L, precision)
+    rhs, vector = op.rhs(B)
+    X = op.entry("cholesky_solve")(op.work, rhs, op.precision, backend)
+    return op.solution(op.cast(X), vector)
 
 
 def lu_solve(LU, piv, B, precision=None, backend="auto"):
     """Solve A x = B given (LU, piv) from :func:`lu`."""
-    l, p, single, dt = _prep(LU, precision, 2)
-    pv = np.ascontiguousarray(np.asarray(piv)[None] if single else piv, dtype=np.int32)
-    vec = np.asarray(B).ndim == (1 if single else 2)
-    X = _fn("lu_solve", l)(l, pv, _rhs(B, l, single), p, backend)
-    X = _finish(X, dt, p)
-    X = X[..., 0] if vec else X
-    return X[0] if single else X
+    op = _Operand(LU, precision)
+    p = np.asarray(piv)
+    p = np.ascontiguousarray(p[None] if op.single else p, dtype=np.int32)
+    rhs, vector = op.rhs(B)
+    X = op.entry("lu_solve")(op.work, p, rhs, op.precision, backend)
+    return op.solution(op.cast(X), vector)
 
 
 def _fused(kind, A, B, precision):
-    a, p, single, dt = _prep(A, precision, 2)
-    if p not in ("fp32", "fp64") or (p == "fp64") != (a.dtype == np.float64):
+    """posv/gesv on the GPU in one pass (A untouched), when the precision is native."""
+    op = _Operand(A, precision)
+    if not op.native():
         return None
-    vec = np.asarray(B).ndim == (1 if single else 2)
-    X, info = _fn(f"{kind}_cuda", a)(a, _rhs(B, a, single))
-    X = X[..., 0] if vec else X
-    return (X[0], info[0]) if single else (X, info)
+    rhs, vector = op.rhs(B)
+    X, info = op.entry(kind + "_cuda")(op.work, rhs)
+    return op.solution(X, vector), (info[0] if op.single else info)
 
 
 def posv(A, B, precision=None, backend="auto"):
@@ -138,8 +153,7 @@ def gesv(A, B, precision=None, backend="auto"):
 
 def round_to(x, precision):
     """Round values to the nearest number representable in ``precision`` (float64 in/out)."""
-    x = np.ascontiguousarray(x, dtype=np.float64)
-    return _core.round_to_f64(x, precision)
+    return _core.round_to_f64(np.ascontiguousarray(x, dtype=np.float64), precision)
 
 
 # ---- mixed precision + iterative refinement ------------------------------------------
@@ -192,6 +206,9 @@ def solve_stream(mats, rhs, kinds, write_factors=False):
     (factors list, pivots list) when write_factors. Factors, pivots, info and X are
     bit-identical to ``posv``/``gesv`` with backend="cuda" on each matrix. The set moves
     through the device in chunks of about 96 MB, so it may exceed device memory.
+    NumPy arrays are pageable host memory: a copy between them and the device returns
+    only when it is done, so from here the chunks run one after another, without the
+    copy/compute overlap that ``stream.solve_host`` reaches on pinned torch tensors.
     """
     import torch
     from . import stream as _stream
