@@ -1,6 +1,7 @@
 """tsdx_cuda_solve_stream_noalloc_f32 (scratch in a fixed device array, no
 allocation) against tsdx_cuda_solve_stream_f32 with caller scratch: two calls in a
-row on different streams of matrices, bit-identical factors, pivots, info and X;
+row on one CUDA stream, each over a different set of matrices, bit-identical
+factors, pivots, info and X; the calls leave the device's memory pool untouched;
 a count above the fixed capacity is rejected before anything runs.
 
 The entry point exists for callers that may not allocate device memory when they
@@ -10,6 +11,8 @@ the first call leaks into its results.
 
 Kept in its own file, named to be collected last, so that it also runs after every
 other test has used the library on the same device."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -59,15 +62,58 @@ def run(entry, A, B, npv, meta, wf):
     return A, B, piv, info
 
 
+class PoolWatch:
+    """High-water mark of the device's default memory pool (cudaMallocAsync's pool),
+    reset before the watched calls: any stream-ordered allocation shows up in it."""
+
+    USED_MEM_HIGH = 0x8  # cudaMemPoolAttrUsedMemHigh
+
+    def __init__(self):
+        self.rt = ctypes.CDLL("libcudart.so.12")
+        self.pool = ctypes.c_void_p()
+        assert self.rt.cudaDeviceGetDefaultMemPool(ctypes.byref(self.pool), torch.cuda.current_device()) == 0
+
+    def reset(self):
+        zero = ctypes.c_uint64(0)
+        assert self.rt.cudaMemPoolSetAttribute(self.pool, self.USED_MEM_HIGH, ctypes.byref(zero)) == 0
+
+    def high(self):
+        v = ctypes.c_uint64(0)
+        assert self.rt.cudaMemPoolGetAttribute(self.pool, self.USED_MEM_HIGH, ctypes.byref(v)) == 0
+        return v.value
+
+
 def test_noalloc_matches_scratch_entry_two_calls_in_a_row():
     for seed, count, wf in ((1, 3000, 1), (2, 1700, 0)):
         A, B, npv, meta = packed(seed, count)
         ref = run("scratch", A, B, npv, meta, wf)
+        watch = PoolWatch()
+        torch.cuda.synchronize()
+        watch.reset()
         got = run("noalloc", A, B, npv, meta, wf)
+        assert watch.high() == 0, "the no-allocation entry point allocated from the device pool"
         assert (got[3] != 99).all()
         for x, y in zip(ref, got):
             assert torch.equal(x.view(torch.int32) if x.dtype == torch.float32 else x,
                                y.view(torch.int32) if y.dtype == torch.float32 else y)
+
+
+def test_pool_watch_sees_a_stream_allocation():
+    """The pool check above can fail: the same solve without caller scratch takes its
+    scratch from the device pool, and the high-water mark shows it."""
+    A, B, npv, meta = packed(3, 500)
+    n, nrhs, kind, aoff, boff, poff = meta
+    piv = torch.zeros(npv, dtype=torch.int32, device="cuda")
+    info = torch.zeros(n.numel(), dtype=torch.int32, device="cuda")
+    watch = PoolWatch()
+    torch.cuda.synchronize()
+    watch.reset()
+    P = capi.ptr
+    rc = capi.call("tsdx_cuda_solve_stream_f32", P(A), P(aoff), P(B), P(boff), P(piv), P(poff), P(info), P(n),
+                   P(nrhs), P(kind), n.numel(), 1, 0, None, 0, capi.stream_ptr())
+    capi.check(rc, "stream without scratch")
+    torch.cuda.synchronize()
+    assert watch.high() > 0
 
 
 def test_noalloc_rejects_count_above_capacity():

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -32,7 +33,7 @@ template <class T> int run_stream(dev::StreamArgs<T> a, void* scratch, long long
 namespace {
 thread_local std::string g_err;
 std::atomic<long long> g_launches{0};
-int g_sms[64] = {0};
+int g_sms[kMaxDevices] = {0};
 }  // namespace
 
 void set_cuda_error(cudaError_t e, const char* what) {
@@ -41,8 +42,16 @@ void set_cuda_error(cudaError_t e, const char* what) {
 void set_error_message(const std::string& msg) { g_err = msg; }
 std::atomic<long long>& launch_counter() { return g_launches; }
 
+int lu_kernel_family() {
+  static const int fam = [] {
+    const char* e = std::getenv("TSDX_LU_KERNEL");
+    return (e && std::string(e) == "reg") ? 2 : 1;
+  }();
+  return fam;
+}
+
 int device_sms(int dev) {
-  if (dev < 0 || dev >= 64) return 148;
+  if (dev < 0 || dev >= kMaxDevices) return 148;
   if (g_sms[dev] == 0) {
     int v = 0;
     if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
@@ -129,7 +138,7 @@ struct DeviceCtx {
   bool init = false;
 };
 std::mutex g_host_mu;
-DeviceCtx g_ctx[64];
+DeviceCtx g_ctx[tsdx::host::kMaxDevices];
 
 int grow(void** p, size_t* cap, size_t need) {
   if (need <= *cap) return 0;
@@ -163,7 +172,7 @@ int run_host(Kind kind, T* A, const int* piv_in, int n, int64_t batch, T* B, int
   if (batch == 0) return TSDX_OK;
   int devi = 0;
   if (cudaGetDevice(&devi) != cudaSuccess) return TSDX_ERR_NODEV;
-  if (devi >= 64) return TSDX_ERR_NODEV;
+  if (devi >= tsdx::host::kMaxDevices) return TSDX_ERR_NODEV;
 
   std::lock_guard<std::mutex> lock(g_host_mu);
   DeviceCtx& ctx = g_ctx[devi];
@@ -375,7 +384,7 @@ struct StreamHostCtx {
   cudaEvent_t rec_sent[kStreamSlots] = {};  // the slot's last record upload has finished
   size_t hcap = 0;
 };
-StreamHostCtx g_stream_ctx[64];
+StreamHostCtx g_stream_ctx[tsdx::host::kMaxDevices];
 
 // record of cnt matrices: aoff, boff, poff (int64), n, nrhs (int32), kind (int8)
 constexpr size_t meta_record_bytes(int64_t cnt) { return (size_t(cnt) * 33 + 255) / 256 * 256; }
@@ -428,7 +437,7 @@ int stream_host_entry(T* A, T* B, int* piv, int* info, const int* n, const int* 
   if (any_b && !B) return TSDX_ERR_NULL;
   int devi = 0;
   if (cudaGetDevice(&devi) != cudaSuccess) return TSDX_ERR_NODEV;
-  if (devi >= 64) return TSDX_ERR_NODEV;
+  if (devi >= tsdx::host::kMaxDevices) return TSDX_ERR_NODEV;
 
   std::lock_guard<std::mutex> lock(tsdx::host::g_host_mu);
   StreamHostCtx& sc = g_stream_ctx[devi];

@@ -16,8 +16,10 @@
 // Scratch: kNoAllocMaxCount matrices at most (262,144; 1 MiB of sort permutation
 // plus 520 bytes of bucket counters). Its device address is looked up once per
 // device with cudaGetSymbolAddress on the first call on that device (that first
-// call must not be made while its stream is being captured). A larger count is
-// rejected with TSDX_ERR_TOO_LARGE before anything is launched.
+// call must not be made while its stream is being captured) and kept for the life
+// of the process: it does not survive cudaDeviceReset, so after a reset of a device
+// this entry point must not be called on it again in the same process. A larger
+// count is rejected with TSDX_ERR_TOO_LARGE before anything is launched.
 //
 // What must start at zero: the per-bucket counters (the first kStreamBuckets ints).
 // Every call zeroes them itself with cudaMemsetAsync on its stream before the
@@ -49,7 +51,7 @@ constexpr long long kNoAllocBytes = tsdx::host::stream_scratch_bytes_of(kNoAlloc
 
 static __device__ __align__(256) int g_stream_scratch[kNoAllocBytes / sizeof(int)];
 
-constexpr int kMaxDevices = 64;
+using tsdx::host::kMaxDevices;
 std::mutex g_mu;
 void* g_addr[kMaxDevices] = {};
 
@@ -57,10 +59,7 @@ int scratch_address(void** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) { tsdx::host::set_cuda_error(e, "cudaGetDevice"); return TSDX_ERR_CUDA; }
-  if (dev < 0 || dev >= kMaxDevices) {
-    tsdx::host::set_error_message("device ordinal above the static scratch table");
-    return TSDX_ERR_CUDA;
-  }
+  if (dev < 0 || dev >= kMaxDevices) return TSDX_ERR_NODEV;  // as every other entry point
   std::lock_guard<std::mutex> lk(g_mu);
   if (!g_addr[dev]) {
     e = cudaGetSymbolAddress(&g_addr[dev], g_stream_scratch);

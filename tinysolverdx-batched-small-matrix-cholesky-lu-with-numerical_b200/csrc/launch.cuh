@@ -10,6 +10,7 @@
 #include "blk.cuh"
 #include "solve.cuh"
 #include "blk3.cuh"
+#include "reg.cuh"
 
 namespace tsdx {
 namespace host {
@@ -22,6 +23,10 @@ void set_cuda_error(cudaError_t e, const char* what);
 std::atomic<long long>& launch_counter();
 
 int device_sms(int dev);
+
+// Per-device tables of the library (workspaces, streams, cached addresses) cover
+// device ordinals [0, kMaxDevices); a higher ordinal is reported as TSDX_ERR_NODEV.
+constexpr int kMaxDevices = 64;
 
 // Compiled padded sizes; a matrix of order n runs in the smallest NP >= n
 // (identity padding is exactly transparent to every result, see common.cuh).
@@ -133,8 +138,35 @@ int launch_blk3(const SolveArgs<T>& a, cudaStream_t st) {
   return 0;
 }
 
+// LU kernel family for padded orders 32 and 64: 1 = shared-memory blocked kernels
+// (blk.cuh / blk3.cuh, the default), 2 = register rows (reg.cuh). Read once from
+// TSDX_LU_KERNEL ("smem" or "reg"); both give bit-identical results.
+int lu_kernel_family();
+
+// One warp per matrix with its rows in registers (reg.cuh). float64 at order 64
+// keeps columns [0, 32) in shared memory; every other case holds whole rows in
+// registers.
+template <class T, int NP, int NRHS>
+int launch_reg(const SolveArgs<T>& a, cudaStream_t st) {
+  constexpr int LC = (sizeof(T) == 8 && NP == 64) ? 32 : 0;
+  using C = dev::RegCfg<T, NP, NRHS, LC>;
+  constexpr int WPC = 1;
+  constexpr int SMEM = WPC * C::MATB;
+  auto kern = dev::reg_kernel<T, NP, NRHS, LC, WPC, 1>;
+  if (int rc = prepare(kern, SMEM)) return rc;
+  const long long ctas = (a.batch + WPC - 1) / WPC;
+  const int grid = grid_for(kern, SMEM, ctas, WPC * 32);
+  kern<<<grid, WPC * 32, SMEM, st>>>(a);
+  launch_counter().fetch_add(1);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) { set_cuda_error(e, "kernel launch"); return -5; }
+  return 0;
+}
+
 template <class T, int NP, int NRHS, bool CHOL>
 int launch_blk(const SolveArgs<T>& a, cudaStream_t st) {
+  if constexpr (!CHOL && (NP == 32 || NP == 64))
+    if (lu_kernel_family() == 2) return launch_reg<T, NP, NRHS>(a, st);
   if constexpr (!CHOL && sizeof(T) == 8 && NP == 64) return launch_blk3<T, NP, NRHS>(a, st);
   if constexpr (!CHOL && sizeof(T) == 8 && NP >= 48) return launch_blk2<T, NP, NRHS>(a, st);
   constexpr int GO = blk_lanes<T, NP, NRHS, CHOL>();

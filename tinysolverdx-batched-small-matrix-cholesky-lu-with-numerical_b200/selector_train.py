@@ -1,6 +1,7 @@
 """Train the precision-tier selector and write its weights (selector_weights.npz).
 
     python selector_train.py [--count 2000000] [--epochs 12] [--out selector_weights.npz]
+    python selector_train.py --calibrate-only [--out selector_weights.npz]
 
 Training set: ``count`` seeded synthetic matrices, n uniform over 8..64, half
 symmetric positive definite (Cholesky) and half general (LU), condition number
@@ -11,7 +12,8 @@ whose refinement converges to a normwise backward error <= 1e-15 within 3
 corrections, by running the refinement kernel itself on every tier. A cost table
 (ns per solve of each tier, per order and kind, measured on this GPU) is stored
 with the weights; the solve policy uses it to pick the cheapest tier at or above
-the predicted one. Features, training forward/backward
+the predicted one; --calibrate-only re-measures that table for the kernels
+built now and keeps the trained network. Features, training forward/backward
 and the Adam updates all run in the library's own kernels. The matrices are
 generated and dropped group by group; only features and labels are kept.
 """
@@ -97,9 +99,19 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=11)
     ap.add_argument("--out", default=str(HERE / "selector_weights.npz"))
+    ap.add_argument("--calibrate-only", action="store_true",
+                    help="keep the network in --out and re-measure only its cost table")
     a = ap.parse_args(argv)
     import torch
     sel = importlib.import_module(PKG + ".selector")
+    if a.calibrate_only:
+        s = sel.Selector.load(a.out)
+        s.cost, s.cost_n = calibrate()
+        s.save(a.out)
+        print(json.dumps({"out": a.out, "cost_ns_per_solve": {
+            int(n): {"spd": [round(v, 1) for v in s.cost[i, 0]], "general": [round(v, 1) for v in s.cost[i, 1]]}
+            for i, n in enumerate(s.cost_n)}}), flush=True)
+        return
     t0 = time.time()
     X, y, _ = dataset(a.count, a.seed)
     counts = torch.bincount(y.long(), minlength=4).cpu().tolist()
