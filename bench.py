@@ -57,18 +57,33 @@ SPECIAL = {
                   "kappa log-uniform [1e1,1e8], RHS count uniform {1,2,4,8}, one graph-captured launch sequence",
     "selector": "learned tier selector evaluation: 1,048,576 matrices, n uniform {8..64}, half SPD / half LU, "
                 "kappa log-uniform [1e0,1e14], 1 RHS, selector tiers + fp64 refinement + fp64 fallback",
-    "ir_fp32_n64": "fixed tier: fp32 factorization + fp64 refinement (tolerance 1e-15, at most 3 corrections, fp64 "
-                   "fallback), n=64 general LU, batch 65,536, 1 RHS, kappa log-uniform [1e1,1e3]",
+    "ir_fp32_n64": "fixed tier (--ir-tier, default fp32) factorization + fp64 refinement (tolerance 1e-15, at most 3 "
+                   "corrections, fp64 fallback), n=64 general LU, batch 65,536, 1 RHS, kappa log-uniform [1e1,1e3]",
 }
 
 
-def describe(name):
-    kind, n, batch, nrhs, dt, klo, khi, zf = WORKLOADS[name]
+def describe(name, batch, world):
+    """The config record of a dense workload; both arms print the same one."""
+    kind, n, _, nrhs, dt, klo, khi, zf = WORKLOADS[name]
     what = "LU with partial pivoting + solve (gesv)" if kind == "gesv" else "Cholesky + solve (posv)"
     return {"workload": f"{what}, {dt}, n={n}, batch {batch}, {nrhs} RHS, kappa log-uniform [{klo:g},{khi:g}]"
                         + (f", {zf:.0%} with one zeroed column" if zf else ""),
-            "kind": kind, "n": n, "batch_per_gpu": batch, "nrhs": nrhs,
-            "l2": "inputs larger than L2 (each step factors a fresh copy of the input stack)"}
+            "kind": kind, "n": n, "batch_per_gpu": batch, "nrhs": nrhs, "global_batch": world * batch,
+            "parallelism": f"batch sharded over {world} GPU(s), no collective",
+            "l2": "inputs larger than L2; every warm-up and timed step works on its own untouched copy of the inputs"}
+
+
+def _matrices():
+    """The package's matrices.py (numpy only) loaded by path, so that the reference
+    arm never imports the package, whose __init__ loads the GPU library."""
+    mod = sys.modules.get("tsdx_bench_matrices")
+    if mod is None:
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("tsdx_bench_matrices", ROOT / PKG_NAME / "matrices.py")
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        sys.modules["tsdx_bench_matrices"] = mod
+    return mod
 
 
 def algorithmic_bytes(kind, n, nrhs, s):
@@ -90,13 +105,32 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def traffic_from_profiles(name):
-    """dram bytes per launch recorded from an ncu capture in profiles/ (or None)."""
-    for p in sorted((ROOT / "profiles").glob(f"*__{name}.md")):
+def traffic_from_profiles(name, kernel):
+    """dram bytes per launch of `kernel` on workload `name`, from the ncu summary
+    profiles/<kernel>__<name>.md (or None when that kernel has no capture)."""
+    p = ROOT / "profiles" / f"{kernel}__{name}.md"
+    if p.exists():
         m = re.search(r"traffic_bytes_per_launch[^:]*:\s*([0-9.eE+]+)", p.read_text())
         if m:
             return float(m.group(1))
     return None
+
+
+def dense_kernel(kind, n, dt):
+    """(file stem, description) of the kernel the library launches for a dense
+    workload: the routing of csrc/launch.cuh (TSDX_LU_KERNEL selects the LU kernel
+    family of orders 25..32 and 57..64)."""
+    reg = os.environ.get("TSDX_LU_KERNEL", "") == "reg"
+    if kind == "gesv" and reg and n in range(25, 33):
+        return "reg_kernel", f"reg_kernel<{dt},NP=32,LC=0> (one warp per matrix, rows in registers)"
+    if kind == "gesv" and reg and n in range(57, 65):
+        lc = 32 if dt == "f64" else 0
+        return "reg_kernel", f"reg_kernel<{dt},NP=64,LC={lc}> (one warp per matrix, rows in registers)"
+    if kind == "gesv" and dt == "f64" and n > 56:
+        return "blk3_kernel", f"blk3_kernel<{dt},NP=64,LU> (two warps per matrix, look-ahead)"
+    if kind == "gesv" and dt == "f64" and n > 40:
+        return "blk2_kernel", f"blk2_kernel<{dt},LU> (two warps per matrix)"
+    return "blk_kernel", f"blk_kernel<{dt},{'LU' if kind == 'gesv' else 'Cholesky'}>"
 
 
 # ---------------------------------------------------------------- clocks (NVML)
@@ -149,61 +183,85 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- CPU reference
-def cpu_reference(kind, n, nrhs, dt, seed, budget_s=12.0):
-    """Times the reference library (compiled from its sources) on a bounded sample
-    of the workload with all host threads. Returns (solves/s, threads, sample)."""
-    from oracle.oracle import Oracle, ref_available, PORT_LIB
-    kindlib = "reference" if ref_available() else "port"
-    O = Oracle(kindlib)
-    threads = os.cpu_count() or 1
+def host_threads():
     try:
-        threads = len(os.sched_getaffinity(0))
+        return len(os.sched_getaffinity(0))
     except Exception:
-        pass
-    O.set_num_threads(threads)
-    M = importlib.import_module(PKG_NAME + ".matrices")
+        return os.cpu_count() or 1
+
+
+def host_inputs(name, batch, seed, distinct=8192):
+    """Host stacks of the workload's distribution for the CPU arms: `distinct` seeded
+    matrices (kappa drawn per matrix, zeroed columns as configured) tiled up to the
+    batch, and N(0,1) right-hand sides."""
+    kind, n, _, nrhs, dt, klo, khi, zf = WORKLOADS[name]
+    M = _matrices()
     rng = np.random.default_rng(seed)
+    d = min(batch, distinct)
+    A = (M.general if kind == "gesv" else M.spd)(rng, d, n, M.log_uniform(rng, d, klo, khi))
+    if zf > 0:
+        M.zero_one_column(rng, A, zf)
     dtype = np.float64 if dt == "f64" else np.float32
-    sample = 2048
-    gen = M.general if kind == "gesv" else M.spd
-    A0 = gen(rng, sample, n, M.log_uniform(rng, sample, 1e1, 1e8)).astype(dtype)
-    B0 = rng.standard_normal((sample, n, nrhs)).astype(dtype)
-    lib = O.lib
-    s = "d" if dt == "f64" else "f"
-    best, total, reps = 0.0, 0.0, 0
-    piv = np.zeros((sample, n), np.int32)
-    info = np.zeros(sample, np.int32)
-    while total < budget_s and reps < 50:
+    A = np.ascontiguousarray(np.tile(A, (-(-batch // d), 1, 1))[:batch], dtype=dtype)
+    B = rng.standard_normal((batch, n, nrhs)).astype(dtype)
+    return A, B
+
+
+class CpuReference:
+    """posv/gesv of the reference library compiled from its sources (oracle/_ref),
+    with every host thread, on a whole host stack per call; the C restatement in
+    oracle/ stands in only where the reference library was not built."""
+
+    def __init__(self):
+        from oracle.oracle import Oracle, ref_available
+        self.kind = "reference" if ref_available() else "port"
+        self.O = Oracle(self.kind)
+        self.threads = host_threads() if self.kind == "reference" else 1
+        self.O.set_num_threads(self.threads)
+
+    def seconds(self, kind, A0, B0):
+        """Time of one call on fresh copies of A0, B0 (the copies are not timed)."""
         A, B = A0.copy(), B0.copy()
+        batch, n, nrhs = B.shape
+        piv = np.zeros((batch, n), np.int32)
+        info = np.zeros(batch, np.int32)
+        s = "d" if A.dtype == np.float64 else "f"
         t0 = time.perf_counter()
-        if kindlib == "reference":
+        if self.kind == "reference":
             if kind == "gesv":
-                fn = getattr(lib, f"ref_gesv_batched_{s}")
-                fn(A.ctypes.data_as(C.c_void_p), n, sample, B.ctypes.data_as(C.c_void_p), nrhs,
-                   piv.ctypes.data_as(C.c_void_p), info.ctypes.data_as(C.c_void_p), 0)
+                getattr(self.O.lib, f"ref_gesv_batched_{s}")(A.ctypes.data_as(C.c_void_p), n, batch,
+                                                             B.ctypes.data_as(C.c_void_p), nrhs,
+                                                             piv.ctypes.data_as(C.c_void_p),
+                                                             info.ctypes.data_as(C.c_void_p), 0)
             else:
-                fn = getattr(lib, f"ref_posv_batched_{s}")
-                fn(A.ctypes.data_as(C.c_void_p), n, sample, B.ctypes.data_as(C.c_void_p), nrhs,
-                   info.ctypes.data_as(C.c_void_p), 0)
+                getattr(self.O.lib, f"ref_posv_batched_{s}")(A.ctypes.data_as(C.c_void_p), n, batch,
+                                                             B.ctypes.data_as(C.c_void_p), nrhs,
+                                                             info.ctypes.data_as(C.c_void_p), 0)
         else:
-            (O.gesv if kind == "gesv" else O.posv)(A, B)
-        dt_ = time.perf_counter() - t0
-        total += dt_
-        reps += 1
-        best = max(best, sample / dt_)
-        if dt_ < 0.25 and sample * 4 <= (1 << 15):
-            # grow the sample until one call is long enough to time
-            sample *= 4
-            A0 = np.concatenate([A0] * 4)
-            B0 = np.concatenate([B0] * 4)
-            piv = np.zeros((sample, n), np.int32)
-            info = np.zeros(sample, np.int32)
-    return best, threads, kindlib, f"{sample} matrices per call, best of {reps} calls (Backend::Auto)"
+            (self.O.gesv if kind == "gesv" else self.O.posv)(A, B)
+        return time.perf_counter() - t0
+
+
+def cpu_reference(name, batch, calls=4):
+    """cpu_baseline record: the reference library on the whole configured batch,
+    one untimed call, then the mean of `calls` timed calls."""
+    kind = WORKLOADS[name][0]
+    ref = CpuReference()
+    if ref.kind != "reference":
+        batch = min(batch, 4096)  # the single-threaded C restatement on a bounded sample
+    A0, B0 = host_inputs(name, batch, 99)
+    ref.seconds(kind, A0, B0)
+    t = [ref.seconds(kind, A0, B0) for _ in range(calls)]
+    v = batch / (sum(t) / len(t))
+    what = "reference library compiled from its sources" if ref.kind == "reference" else "C restatement"
+    return {"value": round(v, 1), "unit": "solves/s", "cores": ref.threads, "kind": ref.kind,
+            "sample": f"{what}, Backend::Auto, the whole batch of {batch} matrices per call "
+                      f"(8192 distinct inputs tiled), mean of {calls} calls after one untimed"}
 
 
 # ---------------------------------------------------------------- GPU arm
 def make_inputs(torch, kind, n, batch, nrhs, dtype, klo, khi, zf, seed, device):
-    M = importlib.import_module(PKG_NAME + ".matrices")
+    M = _matrices()
     A = M.torch_stack("general" if kind == "gesv" else "spd", n, batch, klo, khi, seed, device=device)
     g = torch.Generator(device=device)
     g.manual_seed(seed + 1)
@@ -233,10 +291,19 @@ def run_ours(a):
         batch = a.batch
     dtype = torch.float64 if dt == "f64" else torch.float32
     s = 8 if dt == "f64" else 4
+    cfg = describe(a.workload, batch, world)
     A0, B0 = make_inputs(torch, kind, n, batch, nrhs, dtype, klo, khi, zf, 1234 + rank, device)
-    pool = max(2, min(a.steps + a.warmup, int(a.pool)))
+    # every warm-up and timed step factors its own untouched copy of the inputs, as far
+    # as device memory holds them (the stack of one step is larger than L2)
+    want = a.warmup + a.steps
+    per_copy = A0.numel() * A0.element_size() + B0.numel() * B0.element_size()
+    free, _ = torch.cuda.mem_get_info(device)
+    pool = max(2, min(want, int(0.8 * free) // per_copy, a.pool or want))
     As = [A0.clone() for _ in range(pool)]
     Bs = [B0.clone() for _ in range(pool)]
+    if pool < want:
+        cfg["l2"] = (f"inputs larger than L2 ({per_copy / 1e9:.2f} GB per step); {pool} copies cycled, so the steps "
+                     f"after the first {pool} re-factor an already factored stack")
     piv = torch.zeros(batch, n, dtype=torch.int32, device=device)
     info = torch.zeros(batch, dtype=torch.int32, device=device)
     stream = torch.cuda.current_stream()
@@ -273,6 +340,8 @@ def run_ours(a):
         ms = float(t.item())
     ms_step = ms / a.steps
     value = world * batch / (ms_step * 1e-3)
+    del As, Bs
+    torch.cuda.empty_cache()
 
     # --- end to end through the host-pointer C-ABI call (pinned host buffers) ---
     e2e = None
@@ -286,7 +355,7 @@ def run_ours(a):
         sfx = "f64" if dt == "f64" else "f32"
         tot, reps = 0.0, max(3, min(a.steps, 10))
         for i in range(1 + reps):
-            hA.copy_(A0h)
+            hA.copy_(A0h)  # fresh inputs every call, restored outside the timed region
             hB.copy_(B0h)
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -316,59 +385,129 @@ def run_ours(a):
     peak, src = peaks()
     per_launch = batch * algorithmic_bytes(kind, n, nrhs, s)
     achieved = per_launch / (ms_step * 1e-3) / 1e9
-    traffic = traffic_from_profiles(a.workload)
+    stem, kname = dense_kernel(kind, n, dt)
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-            "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": src,
-            "algorithmic_bytes_per_launch": per_launch,
-            "kernel": (f"blk3_kernel<{dt},NP={n},LU> (two warps per matrix, look-ahead)" if kind == "gesv"
-                       and dt == "f64" and n > 56 else
-                       f"blk2_kernel<{dt},NP={n},LU> (two warps per matrix)" if kind == "gesv" and dt == "f64"
-                       and n > 40 else f"blk_kernel<{dt},NP={n},{'LU' if kind == 'gesv' else 'Cholesky'}>"),
+            "frac": round(achieved / peak, 4), "traffic": traffic_from_profiles(a.workload, stem),
+            "peak_source": src, "algorithmic_bytes_per_launch": per_launch, "kernel": kname,
             "gflops": round(batch * flops(kind, n, nrhs) / (ms_step * 1e-3) / 1e9, 1)}
+
+    # the metric's own comparison (bf16+IR against plain fp64 at equal backward error) on
+    # the mixed-precision configuration, at n = 64 and n = 32
+    ir = None
+    if a.workload == "gesv_f64_n64" and not a.skip_ir:
+        ir = ir_comparison(torch, device, rank)
 
     cpu = None
     if rank == 0 and world == 1 and not a.skip_cpu:
-        v, thr, kindlib, sample = cpu_reference(kind, n, nrhs, dt, 99)
-        cpu = {"value": round(v, 1), "unit": "solves/s", "cores": thr, "kind": kindlib, "sample": sample}
+        cpu = cpu_reference(a.workload, batch)
 
     if rank == 0:
-        cfg = describe(a.workload)
-        cfg["batch_per_gpu"] = batch
-        cfg["global_batch"] = world * batch
-        cfg["parallelism"] = f"batch sharded over {world} GPU(s), no collective"
         out = {"metric": METRIC, "value": round(value, 1), "unit": "solves/s", "n_gpus": world, "steps": a.steps,
                "warmup": a.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": dt, "data": "synthetic", "config": cfg, "roofline": roof,
                "cpu_baseline": cpu, "e2e": _link(e2e), "clocks": clk.summary(), "gpu_launches": int(launches)}
+        if ir is not None:
+            out["ir"] = ir
         print(json.dumps(out), flush=True)
     if world > 1:
         dist.destroy_process_group()
 
 
+IR_CONFIG = ("mixed precision + fp64 iterative refinement (normwise backward error <= 1e-15 within 3 corrections, "
+             "else the plain fp64 kernel), half SPD Cholesky / half general LU, 1 RHS, kappa log-uniform [1e1,1e12]; "
+             "n=64: 131,072 matrices, n=32: 262,144")
+
+
+def ir_comparison(torch, device, rank, reps=3):
+    """The metric's comparison on the mixed-precision configuration: bf16+IR, fp16+IR,
+    fp32+IR, the learned selector's tiers and plain fp64, all on the same inputs, at
+    n = 64 and n = 32. Solves/s: CUDA events around each pass (A stays on the device,
+    x holds b on entry), mean of `reps` passes after one untimed pass, each pass on its
+    own fresh copy of b. Backward error: ||b - A x|| / (||A||_F ||x|| + ||b||) of every
+    returned x, in double-double on the device."""
+    M, dev = _pkg("matrices"), _pkg("device")
+    try:
+        sel = _selector(device)
+    except RuntimeError:
+        sel = None
+    out = {"config": IR_CONFIG, "timing": f"mean of {reps} passes after one untimed pass, CUDA events"}
+    for n, batch in ((64, 131072), (32, 262144)):
+        half = batch // 2
+        parts = []
+        for spd, cnt, seed in ((True, half, 4321 + rank + n), (False, batch - half, 8765 + rank + n)):
+            A = M.torch_stack("spd" if spd else "general", n, cnt, 1e1, 1e12, seed, device=device).contiguous()
+            g = torch.Generator(device=device)
+            g.manual_seed(seed + 1)
+            parts.append((spd, A, torch.randn(cnt, n, generator=g, device=device, dtype=torch.float64)))
+        policies = [("plain_fp64", 3), ("bf16_ir", 1), ("fp16_ir", 0), ("fp32_ir", 2)]
+        if sel is not None:
+            policies.append(("selector", None))
+        pol = {}
+        for name, tier in policies:
+            xs = [[b.clone() for _ in range(reps + 1)] for _, _, b in parts]
+            res = {}
+
+            def run(r):
+                for pi, (spd, A, _) in enumerate(parts):
+                    if tier is None:
+                        res[pi] = sel.solve(A, xs[pi][r], spd)
+                    else:
+                        res[pi] = dev.ir(A, xs[pi][r], spd, default_tier=tier)
+            _once(lambda: run(0))
+            ms = sum(_once(lambda r=r: run(r)) for r in range(1, reps + 1)) / reps
+            bwd = torch.cat([dev.solve_backward_error(A, xs[pi][reps], b) for pi, (_, A, b) in enumerate(parts)])
+            status = torch.cat([res[pi][1] for pi in range(len(parts))])
+            rec = {"solves_per_s": round(batch / (ms * 1e-3), 1), "ms": round(ms, 3), "bwd": _stats(bwd)}
+            if tier is None:
+                t = torch.cat([res[pi][3] for pi in range(len(parts))]).long()
+                rec["tiers"] = dict(zip(("fp16", "bf16", "fp32", "fp64"), torch.bincount(t, minlength=4).tolist()))
+                rec["fp64_fallbacks"] = int(((t < 3) & (status < 0)).sum().item())
+            elif tier < 3:
+                rec["fp64_fallbacks"] = int((status < 0).sum().item())
+            pol[name] = rec
+            del xs, res
+        base = pol["plain_fp64"]
+        out[f"n{n}"] = {
+            "batch": batch, "policies": pol,
+            "speedup_vs_plain_fp64": {k: round(v["solves_per_s"] / base["solves_per_s"], 3)
+                                      for k, v in pol.items() if k != "plain_fp64"},
+            "bwd_max_vs_plain_fp64": {k: round(v["bwd"]["max"] / base["bwd"]["max"], 3)
+                                      for k, v in pol.items() if k != "plain_fp64"}}
+        del parts
+        torch.cuda.empty_cache()
+    return out
+
+
 def run_reference(a):
+    """The reference library (compiled from its sources, all host threads) on the
+    same workload: each step is one call on the whole configured batch, on fresh
+    copies of the inputs made outside the timed region."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     kind, n, batch, nrhs, dt, *_ = WORKLOADS[a.workload]
-    vals = []
-    budget = max(2.0, 150.0 / max(1, a.steps + a.warmup))
-    for i in range(a.warmup + a.steps):
-        v, thr, kindlib, sample = cpu_reference(kind, n, nrhs, dt, 7 + i, budget_s=budget)
-        if i >= a.warmup:
-            vals.append(v)
-    value = float(np.median(vals))
-    cfg = describe(a.workload)
-    cfg["global_batch"] = batch
+    if a.batch:
+        batch = a.batch
+    ref = CpuReference()
+    if ref.kind != "reference":
+        batch = min(batch, 4096)  # the single-threaded C restatement on a bounded sample
+    cfg = describe(a.workload, batch, world)
+    A0, B0 = host_inputs(a.workload, batch, 7)
+    for _ in range(a.warmup):
+        ref.seconds(kind, A0, B0)
+    secs = sum(ref.seconds(kind, A0, B0) for _ in range(a.steps))
+    value = batch * a.steps / secs
+    what = "reference library compiled from its sources" if ref.kind == "reference" else "C restatement"
     out = {"metric": METRIC, "value": round(value, 1), "unit": "solves/s", "n_gpus": world, "steps": a.steps,
-           "warmup": a.warmup, "ms_per_step": round(batch / value * 1e3, 3), "higher_is_better": True,
+           "warmup": a.warmup, "ms_per_step": round(secs / a.steps * 1e3, 3), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": dt, "data": "synthetic", "config": cfg,
            "impl": "reference",
-           "cpu_baseline": {"value": round(value, 1), "unit": "solves/s", "cores": thr, "kind": kindlib,
-                            "sample": sample},
+           "cpu_baseline": {"value": round(value, 1), "unit": "solves/s", "cores": ref.threads, "kind": ref.kind,
+                            "sample": f"{what}, Backend::Auto, one call per step on the whole batch of {batch} "
+                                      f"matrices (8192 distinct inputs tiled)"},
            "e2e": {"value": round(value, 1), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
-
 
 
 # ---------------------------------------------------------------- mixed precision, stream, selector
@@ -676,7 +815,7 @@ def _ir_workload(a, world, rank, local, device, dist):
     bytes_step = batch * (8 * (n * n + 2 * n) + 4)
     routed = "every matrix routed to fp64 by the calibrated policy: blk2_kernel x-only" if tiers.get("fp64") == batch \
         else "ir_kernel<64> + features + mlp_forward + fp64 fallback"
-    roof = _roof(bytes_step, ms, routed, traffic=traffic_from_profiles("ir_n64"))
+    roof = _roof(bytes_step, ms, routed, traffic=traffic_from_profiles("ir_n64", "ir_kernel"))
     # end to end: pinned host A and b in, x and info out, every step
     e2e = None
     if not a.skip_e2e:
@@ -701,10 +840,13 @@ def _ir_workload(a, world, rank, local, device, dist):
     return value, ms, "f64 (tiers fp16/bf16/fp32 factor, fp64 residual)", cfg, roof, cpu, e2e, clk, launches, extra
 
 
-def _stream_workload(a, world, rank, local, device, dist):
+def stream_inputs(count, rank, device):
+    """The uneven stream of the benchmark: n uniform over 2..64, Cholesky (SPD) and LU
+    (general) half each, kappa log-uniform [1e1, 1e8] per matrix, 1, 2, 4 or 8
+    right-hand sides; packed float32 A and B on the device. Returns
+    (n, nrhs, kind, A, B) with n, nrhs, kind as numpy arrays."""
     import torch
     M, stream = _pkg("matrices"), _pkg("stream")
-    count = a.batch or 1048576
     g = np.random.default_rng(1000 + rank)
     n = g.integers(2, 65, count).astype(np.int32)
     kind = g.integers(0, 2, count).astype(np.int8)
@@ -727,6 +869,15 @@ def _stream_workload(a, world, rank, local, device, dist):
     gB = torch.Generator(device=device)
     gB.manual_seed(3000 + rank)
     B0 = torch.randn(nb, generator=gB, dtype=torch.float32, device=device)
+    return n, nrhs, kind, A0, B0
+
+
+def _stream_workload(a, world, rank, local, device, dist):
+    import torch
+    stream = _pkg("stream")
+    count = a.batch or 1048576
+    n, nrhs, kind, A0, B0 = stream_inputs(count, rank, device)
+    aoff, boff, poff, na, nb, npv = stream.layout(n, nrhs)
     plan = stream.StreamPlan(n, nrhs, kind, torch.float32, device=device)
     plan.tune(A0, B0, reps=2)
     pool = max(2, min(a.steps + a.warmup, 11))
@@ -751,7 +902,7 @@ def _stream_workload(a, world, rank, local, device, dist):
     bytes_step = int((4 * (2 * n64 * n64 + 2 * n64 * nrhs) + 4 + np.where(kind == 1, 4 * n64, 0)).sum())
     flops_step = float((np.where(kind == 1, 2 * n64 ** 3 / 3, n64 ** 3 / 3) + 2 * n64 * n64 * nrhs).sum())
     roof = _roof(bytes_step, ms, "stream_kernel<float> x3 drains (+ histogram, scan, scatter)", flops_step,
-                 traffic_from_profiles("stream_f32"))
+                 traffic_from_profiles("stream_f32", "stream_kernel"))
     extra = {"schedule": {"sched_bits": plan.sched, "tuned_ms": {str(k): round(v, 3) for k, v in plan.timings.items()}}}
     e2e = None
     if not a.skip_e2e:
@@ -885,20 +1036,23 @@ def _ir_fixed_workload(a, world, rank, local, device, dist):
     b = torch.randn(batch, n, generator=g, device=device, dtype=torch.float64)
     pool = max(2, min(a.steps + a.warmup, 24))
     xs = [b.clone() for _ in range(pool)]
-    ms, clk, launches = _timed(lambda i: dev.ir(A, xs[i % pool], False, default_tier=2), a, world, local, device, dist)
+    tier = {"fp16": 0, "bf16": 1, "fp32": 2}[a.ir_tier]
+    ms, clk, launches = _timed(lambda i: dev.ir(A, xs[i % pool], False, default_tier=tier), a, world, local, device,
+                               dist)
     value = world * batch / (ms * 1e-3)
     x = b.clone()
-    _, status, _ = dev.ir(A, x, False, default_tier=2)
+    _, status, _ = dev.ir(A, x, False, default_tier=tier)
     xp = b.clone()
     tp = _once(lambda: dev.ir(A, xp, False, default_tier=3))
-    extra = {"refined_without_fallback": float((status >= 0).float().mean().item()),
-             "corrections_median": float(status[status >= 0].float().median().item()),
+    refined = status[status >= 0]
+    extra = {"tier": a.ir_tier, "refined_without_fallback": float((status >= 0).float().mean().item()),
+             "corrections_median": float(refined.float().median().item()) if refined.numel() else None,
              "plain_fp64": {"solves_per_s": round(batch / (tp * 1e-3), 1), "ms": round(tp, 4)},
              "speedup_vs_plain_fp64": round(value / world / (batch / (tp * 1e-3)), 3),
-             "backward_error": {"ir_fp32": _stats(dev.solve_backward_error(A, x, b)),
+             "backward_error": {f"ir_{a.ir_tier}": _stats(dev.solve_backward_error(A, x, b)),
                                 "plain_fp64": _stats(dev.solve_backward_error(A, xp, b))}}
-    roof = _roof(batch * (8 * (n * n + 2 * n) + 4), ms, "ir_kernel<64,LU> (fp32 tier)",
-                 traffic=traffic_from_profiles("ir_fp32_n64"))
+    roof = _roof(batch * (8 * (n * n + 2 * n) + 4), ms, f"ir_kernel<64,LU> ({a.ir_tier} tier)",
+                 traffic=traffic_from_profiles(f"ir_{a.ir_tier}_n64", "ir_kernel"))
     cpu = None
     if rank == 0 and world == 1 and not a.skip_cpu:
         rng = np.random.default_rng(6)
@@ -909,7 +1063,7 @@ def _ir_fixed_workload(a, world, rank, local, device, dist):
     cfg = {"workload": SPECIAL["ir_fp32_n64"], "global_batch": world * batch, "batch_per_gpu": batch,
            "parallelism": f"batch sharded over {world} GPU(s), no collective",
            "l2": "inputs larger than L2 (2.1 GB of A per step)"}
-    return value, ms, "f64 (fp32 factor, fp64 residual)", cfg, roof, cpu, None, clk, launches, extra
+    return value, ms, f"f64 ({a.ir_tier} factor, fp64 residual)", cfg, roof, cpu, None, clk, launches, extra
 
 
 def run_ours_special(a):
@@ -931,7 +1085,7 @@ def run_reference_special(a):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    M = _pkg("matrices")
+    M = _matrices()
     vals = []
     budget = max(2.0, 150.0 / max(1, a.steps + a.warmup))
     rng = np.random.default_rng(9)
@@ -978,7 +1132,11 @@ def main(argv=None):
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="gesv_f64_n64", choices=sorted(WORKLOADS) + sorted(SPECIAL))
     ap.add_argument("--batch", type=int, default=0, help="override the workload's batch (profiling runs)")
-    ap.add_argument("--pool", type=int, default=12, help="distinct input copies cycled through the steps")
+    ap.add_argument("--pool", type=int, default=0,
+                    help="at most this many input copies (default: one per warm-up and timed step)")
+    ap.add_argument("--skip-ir", action="store_true", help="leave out the mixed-precision comparison block")
+    ap.add_argument("--ir-tier", default="fp32", choices=["fp16", "bf16", "fp32"],
+                    help="factorization tier of the ir_fp32_n64 workload")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     a = ap.parse_args(argv)

@@ -67,3 +67,29 @@ def test_reference_arm_under_torchrun_two_ranks():
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] > 0
+
+
+def test_reference_arm_loads_only_the_reference_library():
+    """The reference arm's process maps oracle/_ref/libtsdx_ref.so and none of the
+    package's native libraries (it never imports the package)."""
+    import subprocess
+    import sys
+    if not (ROOT / "oracle" / "_ref" / "libtsdx_ref.so").exists():
+        pytest.skip("oracle/_ref not built")
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--workload', 'posv_f64_n16', "
+            "'--steps', '1', '--warmup', '3', '--batch', '4096']; runpy.run_path('bench.py', run_name='__main__'); "
+            "maps = open('/proc/self/maps').read(); "
+            "print('MAPS', int('libtsdx_ref.so' in maps), int('libtsdx_cuda.so' in maps), int('_core.' in maps), "
+            "int(any('b200' in m for m in sys.modules)))")
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = [ln for ln in out.stdout.splitlines() if ln.startswith("MAPS")][0]
+    assert line.split()[1:] == ["1", "0", "0", "0"], line
+
+
+def test_both_arms_describe_the_same_config():
+    b = _bench()
+    for name in b.WORKLOADS:
+        batch = b.WORKLOADS[name][2]
+        c = b.describe(name, batch, 1)
+        assert c["global_batch"] == batch and c["batch_per_gpu"] == batch and c["parallelism"]
