@@ -118,19 +118,17 @@ def traffic_from_profiles(name, kernel):
 
 def dense_kernel(kind, n, dt):
     """(file stem, description) of the kernel the library launches for a dense
-    workload: the routing of csrc/launch.cuh (TSDX_LU_KERNEL selects the LU kernel
-    family of orders 25..32 and 57..64)."""
-    reg = os.environ.get("TSDX_LU_KERNEL", "") == "reg"
-    if kind == "gesv" and reg and n in range(25, 33):
-        return "reg_kernel", f"reg_kernel<{dt},NP=32,LC=0> (one warp per matrix, rows in registers)"
-    if kind == "gesv" and reg and n in range(57, 65):
-        lc = 32 if dt == "f64" else 0
-        return "reg_kernel", f"reg_kernel<{dt},NP=64,LC={lc}> (one warp per matrix, rows in registers)"
-    if kind == "gesv" and dt == "f64" and n > 56:
+    workload: the routing of csrc/launch.cuh (TSDX_LU_KERNEL=smem or tc forces one
+    LU kernel family)."""
+    fam = os.environ.get("TSDX_LU_KERNEL", "")
+    np_ = next(p for p in (4, 8, 16, 24, 32, 40, 48, 56, 64) if n <= p)
+    if kind == "gesv" and dt == "f64" and np_ >= 32 and (fam == "tc" or (fam != "smem" and np_ <= 48)):
+        return "tc_kernel", f"tc_kernel<NP={np_}> (float64 LU, trailing update on the FP64 tensor cores)"
+    if kind == "gesv" and dt == "f64" and np_ == 64:
         return "blk3_kernel", f"blk3_kernel<{dt},NP=64,LU> (two warps per matrix, look-ahead)"
-    if kind == "gesv" and dt == "f64" and n > 40:
-        return "blk2_kernel", f"blk2_kernel<{dt},LU> (two warps per matrix)"
-    return "blk_kernel", f"blk_kernel<{dt},{'LU' if kind == 'gesv' else 'Cholesky'}>"
+    if kind == "gesv" and dt == "f64" and np_ >= 48:
+        return "blk2_kernel", f"blk2_kernel<{dt},NP={np_},LU> (two warps per matrix)"
+    return "blk_kernel", f"blk_kernel<{dt},NP={np_},{'LU' if kind == 'gesv' else 'Cholesky'}>"
 
 
 # ---------------------------------------------------------------- clocks (NVML)

@@ -45,7 +45,8 @@ std::atomic<long long>& launch_counter() { return g_launches; }
 int lu_kernel_family() {
   static const int fam = [] {
     const char* e = std::getenv("TSDX_LU_KERNEL");
-    return (e && std::string(e) == "reg") ? 2 : 1;
+    const std::string v = e ? e : "";
+    return v == "tc" ? 3 : v == "smem" ? 1 : 0;
   }();
   return fam;
 }

@@ -91,6 +91,48 @@ __device__ __forceinline__ int seg_argmax(unsigned mask, unsigned key, int pos, 
   return __reduce_min_sync(mask, key == mk ? pos : 0x7fffffff);
 }
 
+// Exact warp argmax: the largest key wins, ties go to the smallest position. The
+// first reduction runs on the key's high word; when one lane alone holds that
+// word, it is the winner and no further reduction is needed. *zero: the winning
+// key is 1 (|a| = 0).
+__device__ __forceinline__ int warp_argmax(unsigned long long key, int pos, bool* zero) {
+  const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+  const unsigned mhi = __reduce_max_sync(kFull, hi);
+  const unsigned bal = __ballot_sync(kFull, hi == mhi);
+  if (__popc(bal) == 1) {  // then mhi > 0, so the key is not 1
+    *zero = false;
+    return __shfl_sync(kFull, pos, __ffs(bal) - 1);
+  }
+  const unsigned mlo = __reduce_max_sync(kFull, hi == mhi ? lo : 0u);
+  *zero = (mhi == 0u && mlo == 1u);
+  return __reduce_min_sync(kFull, (hi == mhi && lo == mlo) ? pos : 0x7fffffff);
+}
+__device__ __forceinline__ int warp_argmax(unsigned key, int pos, bool* zero) {
+  const unsigned mk = __reduce_max_sync(kFull, key);
+  *zero = (mk == 1u);
+  const unsigned bal = __ballot_sync(kFull, key == mk);
+  if (__popc(bal) == 1) return __shfl_sync(kFull, pos, __ffs(bal) - 1);
+  return __reduce_min_sync(kFull, key == mk ? pos : 0x7fffffff);
+}
+
+// The same, also returning the winner's lane: the lane whose best candidate is the
+// winning (key, position).
+__device__ __forceinline__ int warp_argmax_lane(unsigned long long key, int pos, bool* zero, int* wl) {
+  const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+  const unsigned mhi = __reduce_max_sync(kFull, hi);
+  const unsigned bal = __ballot_sync(kFull, hi == mhi);
+  if (__popc(bal) == 1) {
+    *zero = false;
+    *wl = __ffs(bal) - 1;
+    return __shfl_sync(kFull, pos, *wl);
+  }
+  const unsigned mlo = __reduce_max_sync(kFull, hi == mhi ? lo : 0u);
+  *zero = (mhi == 0u && mlo == 1u);
+  const int bpos = __reduce_min_sync(kFull, (hi == mhi && lo == mlo) ? pos : 0x7fffffff);
+  *wl = __ffs(__ballot_sync(kFull, pos == bpos)) - 1;
+  return bpos;
+}
+
 // ---- cp.async (LDGSTS) staging of a global byte range into padded rows --------
 template <int VEC>
 __device__ __forceinline__ void cp_async(void* smem, const void* gmem) {

@@ -10,7 +10,7 @@
 #include "blk.cuh"
 #include "solve.cuh"
 #include "blk3.cuh"
-#include "reg.cuh"
+#include "blk_tc.cuh"
 
 namespace tsdx {
 namespace host {
@@ -138,21 +138,21 @@ int launch_blk3(const SolveArgs<T>& a, cudaStream_t st) {
   return 0;
 }
 
-// LU kernel family for padded orders 32 and 64: 1 = shared-memory blocked kernels
-// (blk.cuh / blk3.cuh, the default), 2 = register rows (reg.cuh). Read once from
-// TSDX_LU_KERNEL ("smem" or "reg"); both give bit-identical results.
+// LU kernel family: 0 = by order (the default), 1 = shared-memory blocked kernels
+// with CUDA-core updates everywhere (blk.cuh / blk2.cuh / blk3.cuh), 3 = the float64
+// tensor-core trailing update (blk_tc.cuh) at every padded order 32..64. Read once
+// from TSDX_LU_KERNEL ("smem" or "tc"); all give bit-identical results.
 int lu_kernel_family();
 
-// One warp per matrix with its rows in registers (reg.cuh). float64 at order 64
-// keeps columns [0, 32) in shared memory; every other case holds whole rows in
-// registers.
-template <class T, int NP, int NRHS>
-int launch_reg(const SolveArgs<T>& a, cudaStream_t st) {
-  constexpr int LC = (sizeof(T) == 8 && NP == 64) ? 32 : 0;
-  using C = dev::RegCfg<T, NP, NRHS, LC>;
-  constexpr int WPC = 1;
-  constexpr int SMEM = WPC * C::MATB;
-  auto kern = dev::reg_kernel<T, NP, NRHS, LC, WPC, 1>;
+// float64 LU with the trailing update on the FP64 tensor cores (blk_tc.cuh): a
+// persistent CTA per SM with as many one-matrix warps as shared memory holds.
+template <int NP, int NRHS>
+int launch_tc(const SolveArgs<double>& a, cudaStream_t st) {
+  using C = dev::TcCfg<NP, NRHS>;
+  constexpr int FIT = (227 * 1024) / C::WARPB;
+  constexpr int WPC = FIT < 1 ? 1 : (FIT > 16 ? 16 : FIT);
+  constexpr int SMEM = WPC * C::WARPB;
+  auto kern = dev::tc_kernel<NP, NRHS, WPC>;
   if (int rc = prepare(kern, SMEM)) return rc;
   const long long ctas = (a.batch + WPC - 1) / WPC;
   const int grid = grid_for(kern, SMEM, ctas, WPC * 32);
@@ -165,8 +165,15 @@ int launch_reg(const SolveArgs<T>& a, cudaStream_t st) {
 
 template <class T, int NP, int NRHS, bool CHOL>
 int launch_blk(const SolveArgs<T>& a, cudaStream_t st) {
-  if constexpr (!CHOL && (NP == 32 || NP == 64))
-    if (lu_kernel_family() == 2) return launch_reg<T, NP, NRHS>(a, st);
+  // float64 LU, padded orders 32..48: the tensor-core trailing update, measured on
+  // B200 (65,536-262,144 matrices, 4 right-hand sides) against the shared-memory
+  // kernels: n=25 79.0 vs 68.1, n=32 75.6 vs 65.3, n=40 37.6 vs 33.3, n=48 24.6 vs
+  // 23.1 M solves/s; slower at 56..64 (one warp per matrix, 6 per SM, against two)
+  if constexpr (!CHOL && sizeof(T) == 8 && NP >= 32) {
+    const int fam = lu_kernel_family();
+    if (fam == 3 || (fam == 0 && NP <= 48))
+      return launch_tc<NP, NRHS>(reinterpret_cast<const SolveArgs<double>&>(a), st);
+  }
   if constexpr (!CHOL && sizeof(T) == 8 && NP == 64) return launch_blk3<T, NP, NRHS>(a, st);
   if constexpr (!CHOL && sizeof(T) == 8 && NP >= 48) return launch_blk2<T, NP, NRHS>(a, st);
   constexpr int GO = blk_lanes<T, NP, NRHS, CHOL>();
