@@ -122,7 +122,7 @@ def dense_kernel(kind, n, dt):
     LU kernel family)."""
     fam = os.environ.get("TSDX_LU_KERNEL", "")
     np_ = next(p for p in (4, 8, 16, 24, 32, 40, 48, 56, 64) if n <= p)
-    if kind == "gesv" and dt == "f64" and np_ >= 32 and (fam == "tc" or (fam != "smem" and np_ <= 48)):
+    if kind == "gesv" and dt == "f64" and np_ >= 32 and (fam == "tc" or (fam != "smem" and (np_ <= 48 or n % 2 == 0))):
         return "tc_kernel", f"tc_kernel<NP={np_}> (float64 LU, trailing update on the FP64 tensor cores)"
     if kind == "gesv" and dt == "f64" and np_ == 64:
         return "blk3_kernel", f"blk3_kernel<{dt},NP=64,LU> (two warps per matrix, look-ahead)"

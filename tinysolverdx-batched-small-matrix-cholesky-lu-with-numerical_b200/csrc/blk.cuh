@@ -103,6 +103,18 @@ __device__ __forceinline__ void seg_copy_out(const unsigned char* M, T* A, int n
   const int vec = vec_of<T>(A, n);
   const int rc = n * int(sizeof(T)) / vec;
   char* g = reinterpret_cast<char*>(A);
+  if (vec == 16 && rc <= G && G % rc == 0) {
+    // one 16-byte chunk per lane and row, G / rc rows per pass; the passes are
+    // independent, so unrolled they keep several loads in flight
+    const int rpp = G / rc, c = lsl % rc;
+#pragma unroll 4
+    for (int k = lsl / rc; k < n; k += rpp) {
+      const unsigned char* sr = M + (src ? src[k] : k) * RS;
+      *reinterpret_cast<uint4*>(g + (long long)k * n * int(sizeof(T)) + c * 16) =
+          *reinterpret_cast<const uint4*>(sr + c * 16);
+    }
+    return;
+  }
   for (int k = 0; k < n; ++k) {
     const unsigned char* sr = M + (src ? src[k] : k) * RS;
     char* gr = g + (long long)k * n * int(sizeof(T));
@@ -147,17 +159,23 @@ __device__ __forceinline__ void seg_backsolve(unsigned char* M, const int* ord, 
   constexpr int G = C::G, MR = C::MR, RS = C::RS;
   auto at = [&](int r, int c) -> T& { return *reinterpret_cast<T*>(M + r * RS + c * int(sizeof(T))); };
   T yv[MR][NRHS], dv[MR];
+  // U(i, k) of this lane's rows at ubase[t] + k * ustride (LU: row ord[i], column k;
+  // Cholesky: row k, column i)
+  const unsigned char* ubase[MR];
+  constexpr int ustride = CHOL ? RS : int(sizeof(T));
 #pragma unroll
   for (int t = 0; t < MR; ++t) {
     const int i = g.lsl + G * t;
     const int ii = i < NP ? i : 0;
     const int pr = CHOL ? ii : ord[ii];
     dv[t] = rcp_(at(pr, ii));
+    ubase[t] = CHOL ? M + ii * int(sizeof(T)) : M + pr * RS;
 #pragma unroll
     for (int c = 0; c < NRHS; ++c) yv[t][c] = at(pr, NP + c);
   }
   // a warp-uniform trip count (segments of one warp may hold different n); the
   // identity-padded positions >= n carry zeros and change nothing
+#pragma unroll 4
   for (int k = NP - 1; k >= 0; --k) {
     const int ks = k / G, kl = g.segbase + (k & (G - 1));
     T x[NRHS];
@@ -169,16 +187,16 @@ __device__ __forceinline__ void seg_backsolve(unsigned char* M, const int* ord, 
         if (ks == t) y = yv[t][c] * dv[t];
       x[c] = __shfl_sync(kFull, y, kl);
     }
+    // branch-free: rows above k take the update, row k takes x, rows below keep y
+    // (U is read for every row; the address is inside the matrix)
 #pragma unroll
     for (int t = 0; t < MR; ++t) {
       const int i = g.lsl + G * t;
-      if (i < k) {
-        const T u = CHOL ? at(k, i) : at(ord[i], k);
+      const T u = *reinterpret_cast<const T*>(ubase[t] + k * ustride);
 #pragma unroll
-        for (int c = 0; c < NRHS; ++c) yv[t][c] = fma_(-u, x[c], yv[t][c]);
-      } else if (i == k) {
-#pragma unroll
-        for (int c = 0; c < NRHS; ++c) yv[t][c] = x[c];
+      for (int c = 0; c < NRHS; ++c) {
+        const T upd = fma_(-u, x[c], yv[t][c]);
+        yv[t][c] = i < k ? upd : (i == k ? x[c] : yv[t][c]);
       }
     }
   }

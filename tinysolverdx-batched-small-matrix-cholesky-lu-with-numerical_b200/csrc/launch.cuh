@@ -165,13 +165,15 @@ int launch_tc(const SolveArgs<double>& a, cudaStream_t st) {
 
 template <class T, int NP, int NRHS, bool CHOL>
 int launch_blk(const SolveArgs<T>& a, cudaStream_t st) {
-  // float64 LU, padded orders 32..48: the tensor-core trailing update, measured on
-  // B200 (65,536-262,144 matrices, 4 right-hand sides) against the shared-memory
-  // kernels: n=25 79.0 vs 68.1, n=32 75.6 vs 65.3, n=40 37.6 vs 33.3, n=48 24.6 vs
-  // 23.1 M solves/s; slower at 56..64 (one warp per matrix, 6 per SM, against two)
+  // float64 LU from padded order 32 on: the tensor-core trailing update. Measured on
+  // B200 against the shared-memory kernels (65,536-262,144 matrices, 4 right-hand
+  // sides, M solves/s): n=25 77.1 vs 68.1, n=32 93.0 vs 65.3, n=40 38.0 vs 33.3,
+  // n=48 26.8 vs 23.1, n=56 18.2 vs 16.7, n=64 15.3 vs 12.9. Odd orders above 48
+  // stay on the shared-memory kernels (n=61 11.6 vs 12.3): their rows are not whole
+  // 16-byte units, so the matrix cannot arrive by bulk copies.
   if constexpr (!CHOL && sizeof(T) == 8 && NP >= 32) {
     const int fam = lu_kernel_family();
-    if (fam == 3 || (fam == 0 && NP <= 48))
+    if (fam == 3 || (fam == 0 && (NP <= 48 || a.n % 2 == 0)))
       return launch_tc<NP, NRHS>(reinterpret_cast<const SolveArgs<double>&>(a), st);
   }
   if constexpr (!CHOL && sizeof(T) == 8 && NP == 64) return launch_blk3<T, NP, NRHS>(a, st);
