@@ -420,9 +420,11 @@ def ir_comparison(torch, device, rank, reps=3):
     """The metric's comparison on the mixed-precision configuration: bf16+IR, fp16+IR,
     fp32+IR, the learned selector's tiers and plain fp64, all on the same inputs, at
     n = 64 and n = 32. Solves/s: CUDA events around each pass (A stays on the device,
-    x holds b on entry), mean of `reps` passes after one untimed pass, each pass on its
-    own fresh copy of b. Backward error: ||b - A x|| / (||A||_F ||x|| + ||b||) of every
-    returned x, in double-double on the device."""
+    x holds b on entry), mean of `reps` passes after one untimed pass per policy, each
+    pass on its own fresh copy of b; the timed passes go round the policies in turn, so
+    a drift of the clocks over the run falls on every policy alike. Backward error:
+    ||b - A x|| / (||A||_F ||x|| + ||b||) of every returned x, in double-double on the
+    device."""
     M, dev = _pkg("matrices"), _pkg("device")
     try:
         sel = _selector(device)
@@ -440,30 +442,35 @@ def ir_comparison(torch, device, rank, reps=3):
         policies = [("plain_fp64", 3), ("bf16_ir", 1), ("fp16_ir", 0), ("fp32_ir", 2)]
         if sel is not None:
             policies.append(("selector", None))
+        xs = {name: [[b.clone() for _ in range(reps + 1)] for _, _, b in parts] for name, _ in policies}
+        res = {name: {} for name, _ in policies}
+
+        def run(name, tier, r):
+            for pi, (spd, A, _) in enumerate(parts):
+                if tier is None:
+                    res[name][pi] = sel.solve(A, xs[name][pi][r], spd)
+                else:
+                    res[name][pi] = dev.ir(A, xs[name][pi][r], spd, default_tier=tier)
+        for name, tier in policies:
+            _once(lambda: run(name, tier, 0))
+        total = {name: 0.0 for name, _ in policies}
+        for r in range(1, reps + 1):
+            for name, tier in policies:
+                total[name] += _once(lambda: run(name, tier, r))
         pol = {}
         for name, tier in policies:
-            xs = [[b.clone() for _ in range(reps + 1)] for _, _, b in parts]
-            res = {}
-
-            def run(r):
-                for pi, (spd, A, _) in enumerate(parts):
-                    if tier is None:
-                        res[pi] = sel.solve(A, xs[pi][r], spd)
-                    else:
-                        res[pi] = dev.ir(A, xs[pi][r], spd, default_tier=tier)
-            _once(lambda: run(0))
-            ms = sum(_once(lambda r=r: run(r)) for r in range(1, reps + 1)) / reps
-            bwd = torch.cat([dev.solve_backward_error(A, xs[pi][reps], b) for pi, (_, A, b) in enumerate(parts)])
-            status = torch.cat([res[pi][1] for pi in range(len(parts))])
+            ms = total[name] / reps
+            bwd = torch.cat([dev.solve_backward_error(A, xs[name][pi][reps], b) for pi, (_, A, b) in enumerate(parts)])
+            status = torch.cat([res[name][pi][1] for pi in range(len(parts))])
             rec = {"solves_per_s": round(batch / (ms * 1e-3), 1), "ms": round(ms, 3), "bwd": _stats(bwd)}
             if tier is None:
-                t = torch.cat([res[pi][3] for pi in range(len(parts))]).long()
+                t = torch.cat([res[name][pi][3] for pi in range(len(parts))]).long()
                 rec["tiers"] = dict(zip(("fp16", "bf16", "fp32", "fp64"), torch.bincount(t, minlength=4).tolist()))
                 rec["fp64_fallbacks"] = int(((t < 3) & (status < 0)).sum().item())
             elif tier < 3:
                 rec["fp64_fallbacks"] = int((status < 0).sum().item())
             pol[name] = rec
-            del xs, res
+        del xs, res
         base = pol["plain_fp64"]
         out[f"n{n}"] = {
             "batch": batch, "policies": pol,

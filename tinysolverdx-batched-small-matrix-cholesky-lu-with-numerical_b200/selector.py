@@ -88,12 +88,18 @@ class Selector:
     # (fp16 carries more precision than bf16 once the matrix is scaled into range)
     CANDIDATES = {0: (0, 2, 3), 1: (1, 0, 2, 3), 2: (2, 3), 3: (3,)}
 
+    # a lower tier runs only when its cost (features and network included) is below
+    # this fraction of the fp64 cost: the table is measured at kappa <= 10, where every
+    # tier converges in few corrections, and a routed batch takes one more launch
+    ROUTE_MARGIN = 0.9
+
     def policy_lut(self, n, spd):
         """int8 (4,) map from predicted tier to the tier to run for order n and kind."""
         lut = np.arange(4, dtype=np.int8)
         if self.cost is not None:
             i = int(np.argmin(np.abs(np.asarray(self.cost_n) - n)))
-            c = self.cost[i, 0 if spd else 1]
+            c = np.array(self.cost[i, 0 if spd else 1], dtype=np.float64)
+            c[:3] = np.where(c[:3] <= self.ROUTE_MARGIN * c[3], c[:3], np.inf)
             for t, cand in self.CANDIDATES.items():
                 lut[t] = min(cand, key=lambda u: c[u])
         return lut

@@ -63,13 +63,15 @@ def dataset(count, seed, device="cuda", sizes=SIZES, kappa=(1e0, 1e14), keep=Fal
     return torch.cat(Xs), torch.cat(ys), groups
 
 
-def calibrate(device="cuda", sizes=(8, 16, 24, 32, 40, 48, 56, 64), count=16384, reps=3):
+def calibrate(device="cuda", sizes=(8, 16, 24, 32, 40, 48, 56, 64), count=16384, reps=3, sel=None):
     """Measured ns per solve of each tier on well-conditioned matrices (kappa <= 10,
     where every tier converges): cost[size][kind (0 SPD, 1 general)][tier], tier 3 =
-    the plain fp64 solve. CUDA events, best of ``reps``."""
+    the plain fp64 solve. The lower tiers include the selector's own pass (features
+    and network forward) when ``sel`` is given. CUDA events, best of ``reps``."""
     import torch
     M = importlib.import_module(PKG + ".matrices")
     dev = importlib.import_module(PKG + ".device")
+    selm = importlib.import_module(PKG + ".selector")
     cost = np.zeros((len(sizes), 2, 4))
     for i, n in enumerate(sizes):
         for kd, spd in ((0, True), (1, False)):
@@ -88,6 +90,17 @@ def calibrate(device="cuda", sizes=(8, 16, 24, 32, 40, 48, 56, 64), count=16384,
                     e1.synchronize()
                     best = min(best, e0.elapsed_time(e1))
                 cost[i, kd, t] = best * 1e6 / count
+            if sel is not None:
+                best = float("inf")
+                for _ in range(reps + 1):
+                    torch.cuda.synchronize()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    sel.predict(selm.features(A, kd))
+                    e1.record()
+                    e1.synchronize()
+                    best = min(best, e0.elapsed_time(e1))
+                cost[i, kd, :3] += best * 1e6 / count
     return cost, np.asarray(sizes)
 
 
@@ -106,7 +119,7 @@ def main(argv=None):
     sel = importlib.import_module(PKG + ".selector")
     if a.calibrate_only:
         s = sel.Selector.load(a.out)
-        s.cost, s.cost_n = calibrate()
+        s.cost, s.cost_n = calibrate(sel=s)
         s.save(a.out)
         print(json.dumps({"out": a.out, "cost_ns_per_solve": {
             int(n): {"spd": [round(v, 1) for v in s.cost[i, 0]], "general": [round(v, 1) for v in s.cost[i, 1]]}
@@ -121,7 +134,7 @@ def main(argv=None):
     torch.cuda.synchronize()
     t2 = time.time()
     acc = (s.predict(X) == y).float().mean().item()
-    s.cost, s.cost_n = calibrate()
+    s.cost, s.cost_n = calibrate(sel=s)
     s.save(a.out)
     print(json.dumps({"count": a.count, "label_counts": dict(zip(sel.TIERS, counts)), "epochs": a.epochs,
                       "loss": [round(v, 4) for v in hist], "train_accuracy": round(acc, 4),
