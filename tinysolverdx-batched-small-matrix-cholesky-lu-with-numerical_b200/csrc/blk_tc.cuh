@@ -6,9 +6,9 @@
 // Per panel of 8 columns (k0 = 0, 8, ...):
 //   1. pivot steps in registers (lane l holds rows l and l + 32): argmax of |a| by a
 //      warp reduction on the high word of the key (exact tie-break only when two
-//      lanes share it), the winner's remaining panel row broadcast by shuffles,
-//      multipliers through a shared correctly rounded reciprocal, rank-1 update of
-//      the panel;
+//      lanes share it), the winner's remaining panel row, reciprocal and position
+//      published in a shared-memory record, multipliers through that correctly
+//      rounded reciprocal, rank-1 update of the panel;
 //   2. U12: the panel's pivot rows on the trailing columns, one lane per column;
 //   3. trailing update A22 -= L21 U12 on 8 x 8 tiles: tile (I, J) covers logical
 //      positions j1 + 8I .. j1 + 8I + 7 (gathered through the position -> physical
@@ -100,7 +100,7 @@ struct TcCfg {
 // columns k0 + fq and k0 + 4 + fq; B fragment (k = fq, column fr): the pivot rows of
 // those steps (a zero-pivot step: a = -0, b = +0). NTI == 0: only the right-hand
 // sides are left, and they have no active row.
-template <int NP, int NRHS, int NTI>
+template <int NP, int NRHS, int NTI, bool ZB>
 __device__ __forceinline__ void tc_tiles(unsigned char* M, const int* ord, const int* pmap, unsigned zb, int k0,
                                          int lane) {
   if constexpr (NTI > 0) {
@@ -109,7 +109,7 @@ __device__ __forceinline__ void tc_tiles(unsigned char* M, const int* ord, const
     const int fr = lane >> 2, fq = lane & 3, j1 = k0 + 8;
     auto at = [&](int r, int c) -> double& { return *reinterpret_cast<double*>(M + r * RS + c * 8); };
     auto vat = [&](int r, int c) -> double2& { return *reinterpret_cast<double2*>(M + r * RS + c * 8); };
-    const bool za = (zb >> fq) & 1u, zc = (zb >> (4 + fq)) & 1u;
+    const bool za = ZB && ((zb >> fq) & 1u), zc = ZB && ((zb >> (4 + fq)) & 1u);
     int prow[NTI];
     double a0[NTI], a1[NTI];
 #pragma unroll
@@ -136,6 +136,137 @@ __device__ __forceinline__ void tc_tiles(unsigned char* M, const int* ord, const
   }
 }
 
+// U12 (the panel's pivot rows on the trailing columns, one lane per column) and the
+// trailing update A22 -= L21 U12 on the tensor cores, for the panel at k0. ZB: the
+// panel had a zero-pivot step, which enters both as fma(-(+0), +0, acc) == acc.
+template <int NP, int NRHS, bool ZB>
+__device__ __forceinline__ void tc_update(unsigned char* M, const int* ord, const int* pmap, unsigned zb, int k0,
+                                          int lane) {
+  using C = TcCfg<NP, NRHS>;
+  using T = double;
+  constexpr int PB = C::PB, NC = C::NC, RS = C::RS;
+  const int j1 = k0 + PB;
+  {
+    int prs[PB];
+#pragma unroll
+    for (int i = 0; i < PB; ++i) prs[i] = ord[k0 + i] * RS;
+    T l11[PB][PB];
+#pragma unroll
+    for (int i = 1; i < PB; ++i)
+#pragma unroll
+      for (int i2 = 0; i2 < i; ++i2)
+        l11[i][i2] = (ZB && ((zb >> i2) & 1u)) ? 0.0 : *reinterpret_cast<const T*>(M + prs[i] + (k0 + i2) * 8);
+    if (NC - j1 > 32) {
+      // two columns per lane, interleaved: two independent chains
+      const int jc0 = j1 + lane, jc1 = jc0 + 32;
+      const bool two = jc1 < NC;
+      T uz0[PB], uz1[PB];
+#pragma unroll
+      for (int i = 0; i < PB; ++i) {
+        T* c0 = reinterpret_cast<T*>(M + prs[i] + jc0 * 8);
+        T* c1 = reinterpret_cast<T*>(M + prs[i] + (two ? jc1 : jc0) * 8);
+        T a0 = *c0, a1 = *c1;
+#pragma unroll
+        for (int i2 = 0; i2 < i; ++i2) {
+          a0 = fma_(-l11[i][i2], uz0[i2], a0);
+          a1 = fma_(-l11[i][i2], uz1[i2], a1);
+        }
+        uz0[i] = (ZB && ((zb >> i) & 1u)) ? 0.0 : a0;
+        uz1[i] = (ZB && ((zb >> i) & 1u)) ? 0.0 : a1;
+        if (i > 0) {
+          *c0 = a0;
+          if (two) *c1 = a1;
+        }
+      }
+    } else {
+      const int jc = j1 + lane;
+      if (jc < NC) {
+        T uz[PB];
+#pragma unroll
+        for (int i = 0; i < PB; ++i) {
+          T* cell = reinterpret_cast<T*>(M + prs[i] + jc * 8);
+          T acc = *cell;
+#pragma unroll
+          for (int i2 = 0; i2 < i; ++i2) acc = fma_(-l11[i][i2], uz[i2], acc);
+          uz[i] = (ZB && ((zb >> i) & 1u)) ? 0.0 : acc;
+          if (i > 0) *cell = acc;
+        }
+      }
+    }
+  }
+  __syncwarp();
+  switch ((NP - j1) / 8) {
+    case 7: tc_tiles<NP, NRHS, 7, ZB>(M, ord, pmap, zb, k0, lane); break;
+    case 6: tc_tiles<NP, NRHS, 6, ZB>(M, ord, pmap, zb, k0, lane); break;
+    case 5: tc_tiles<NP, NRHS, 5, ZB>(M, ord, pmap, zb, k0, lane); break;
+    case 4: tc_tiles<NP, NRHS, 4, ZB>(M, ord, pmap, zb, k0, lane); break;
+    case 3: tc_tiles<NP, NRHS, 3, ZB>(M, ord, pmap, zb, k0, lane); break;
+    case 2: tc_tiles<NP, NRHS, 2, ZB>(M, ord, pmap, zb, k0, lane); break;
+    case 1: tc_tiles<NP, NRHS, 1, ZB>(M, ord, pmap, zb, k0, lane); break;
+    default: tc_tiles<NP, NRHS, 0, ZB>(M, ord, pmap, zb, k0, lane); break;
+  }
+  __syncwarp();
+}
+
+// y <- fma(-u, x, y) when p, else y unchanged: one predicated FMA (no select).
+__device__ __forceinline__ void fma_if(double& y, bool p, double u, double x) {
+  asm("{\n .reg .pred q;\n setp.ne.b32 q, %1, 0;\n @q fma.rn.f64 %0, %2, %3, %0;\n}"
+      : "+d"(y)
+      : "r"((int)p), "d"(-u), "d"(x));
+}
+
+// Back substitution over physical rows: lane l solves its rows l and l + 32 (at
+// positions pos[s]) with the right-hand sides that the factorization left in the
+// augmented columns. Step k (from the last position down): the row at position k
+// computes x_k = y_k * RN(1/u_kk) and broadcasts it; rows at positions below k take
+// y <- fma(-u(row, k), x_k, y) (predicated). A row's y is final after its own step,
+// so every row forms its x = y * RN(1/u_kk) once more at the end, the same product.
+// These are the operations of a column-oriented back substitution over positions,
+// without its per-step selects.
+template <int NP, int NRHS>
+__device__ __forceinline__ void tc_backsolve(const unsigned char* M, const int* ord, const int (&pos)[TcCfg<NP, NRHS>::MR],
+                                             const MatJob<double>& j, int lane) {
+  using C = TcCfg<NP, NRHS>;
+  constexpr int MR = C::MR, RS = C::RS;
+  double y[MR][NRHS], dv[MR];
+  const unsigned char* rowp[MR];
+#pragma unroll
+  for (int s = 0; s < MR; ++s) {
+    const int r = lane + 32 * s;
+    const int rr = r < NP ? r : 0;
+    rowp[s] = M + rr * RS;
+    dv[s] = rcp_(*reinterpret_cast<const double*>(rowp[s] + (r < NP ? pos[s] : 0) * 8));
+#pragma unroll
+    for (int c = 0; c < NRHS; ++c) y[s][c] = *reinterpret_cast<const double*>(rowp[s] + (NP + c) * 8);
+  }
+#pragma unroll 4
+  for (int k = NP - 1; k >= 0; --k) {
+    const int po = ord[k];
+    const bool mine0 = MR == 1 || pos[0] == k;
+    const double d = mine0 ? dv[0] : dv[MR - 1];
+    double x[NRHS];
+#pragma unroll
+    for (int c = 0; c < NRHS; ++c) x[c] = __shfl_sync(kFull, (mine0 ? y[0][c] : y[MR - 1][c]) * d, po & 31);
+#pragma unroll
+    for (int s = 0; s < MR; ++s) {
+      const double u = *reinterpret_cast<const double*>(rowp[s] + k * 8);
+      const bool below = pos[s] < k;
+#pragma unroll
+      for (int c = 0; c < NRHS; ++c) fma_if(y[s][c], below, u, x[c]);
+    }
+  }
+  if (j.live && j.B) {
+#pragma unroll
+    for (int s = 0; s < MR; ++s) {
+      if (pos[s] >= j.n) continue;
+      double* brow = j.B + (long long)pos[s] * j.ldb + j.b0;
+#pragma unroll
+      for (int c = 0; c < NRHS; ++c)
+        if (c < j.nrhs) brow[c] = y[s][c] * dv[s];
+    }
+  }
+}
+
 // Returns false when the bulk load of the matrix did not complete (the matrix is then
 // left unsolved with info = -1).
 template <int NP, int NRHS>
@@ -148,11 +279,6 @@ __device__ __forceinline__ bool lu_tc_matrix(unsigned char* M, const MatJob<doub
   int* pmap = pvs + NP;
   auto at = [&](int r, int c) -> T& { return *reinterpret_cast<T*>(M + r * RS + c * 8); };
   auto vat = [&](int r, int c) -> double2& { return *reinterpret_cast<double2*>(M + r * RS + c * 8); };
-  Seg g;
-  g.lane = lane;
-  g.lsl = lane;
-  g.segbase = 0;
-  g.segmask = kFull;
 
   // ---- stage A and, while it lands, the right-hand sides in registers; identity
   // padding up to NP; the columns that pad the right-hand sides to a whole tile take
@@ -249,17 +375,9 @@ __device__ __forceinline__ bool lu_tc_matrix(unsigned char* M, const MatJob<doub
       }
       const unsigned hi = (unsigned)(bk >> 32);
       const unsigned mhi = __reduce_max_sync(kFull, hi);
-      // while the reduction runs: this lane's best row and the reciprocal of its
-      // candidate (the winner publishes both)
-      T brow[PB];
-#pragma unroll
-      for (int jj = i; jj < PB; ++jj) {
-        T v = pan[0][jj];
-#pragma unroll
-        for (int s = 1; s < MR; ++s) v = (bs == s) ? pan[s][jj] : v;
-        brow[jj] = v;
-      }
-      const T rcand = rcp_(brow[i]);
+      // while the reduction runs: the reciprocal of this lane's candidate (the winner
+      // publishes it with its row)
+      const T rcand = rcp_((MR > 1 && bs) ? pan[MR - 1][i] : pan[0][i]);
       const unsigned bal = __ballot_sync(kFull, hi == mhi);
       int wl;
       bool zero;
@@ -279,8 +397,12 @@ __device__ __forceinline__ bool lu_tc_matrix(unsigned char* M, const MatJob<doub
       static_assert(NP * 4 >= 10 * 8, "the record fits the position map");
       if (lane == wl) {
 #pragma unroll
-        for (int jj = i & ~1; jj < PB; jj += 2)
-          *reinterpret_cast<double2*>(rec + jj) = make_double2(jj < i ? 0.0 : brow[jj], brow[jj + 1]);
+        for (int s = 0; s < MR; ++s) {  // stored from the candidate's slot: predicated stores, no selects
+          if (bs != s) continue;
+#pragma unroll
+          for (int jj = i & ~1; jj < PB; jj += 2)
+            *reinterpret_cast<double2*>(rec + jj) = make_double2(pan[s][jj], pan[s][jj + 1]);
+        }
         rec[8] = rcand;
         reinterpret_cast<int*>(rec + 9)[0] = bp;
         ord[k] = lane + 32 * bs;
@@ -300,9 +422,8 @@ __device__ __forceinline__ bool lu_tc_matrix(unsigned char* M, const MatJob<doub
       // retire the winner and replay the reference's swap of positions k and bpos
 #pragma unroll
       for (int s = 0; s < MR; ++s) {
-        const bool win = act[s] && pos[s] == bpos;
-        const bool atk = act[s] && !win && pos[s] == k;
-        pos[s] = win ? k : (atk ? bpos : pos[s]);
+        const bool win = pos[s] == bpos;  // retired rows hold positions below k <= bpos
+        pos[s] = win ? k : (pos[s] == k ? bpos : pos[s]);
         act[s] = act[s] && !win;
       }
       info = (zero && info == 0) ? k + 1 : info;
@@ -351,47 +472,14 @@ __device__ __forceinline__ bool lu_tc_matrix(unsigned char* M, const MatJob<doub
     __syncwarp();
     const int j1 = k0 + PB;
     if (j1 >= NC) continue;
-    // ------------------------------- 2. U12: pivot rows on the trailing columns
-    // branch-free: a zero-pivot step enters as fma(-(+0), +0, acc) == acc
-    {
-      int prs[PB];
-#pragma unroll
-      for (int i = 0; i < PB; ++i) prs[i] = ord[k0 + i] * RS;
-      T l11[PB][PB];
-#pragma unroll
-      for (int i = 1; i < PB; ++i)
-#pragma unroll
-        for (int i2 = 0; i2 < i; ++i2)
-          l11[i][i2] = ((zb >> i2) & 1u) ? 0.0 : *reinterpret_cast<const T*>(M + prs[i] + (k0 + i2) * 8);
-      for (int jc = j1 + lane; jc < NC; jc += 32) {
-        T uz[PB];
-#pragma unroll
-        for (int i = 0; i < PB; ++i) {
-          T* cell = reinterpret_cast<T*>(M + prs[i] + jc * 8);
-          T acc = *cell;
-#pragma unroll
-          for (int i2 = 0; i2 < i; ++i2) acc = fma_(-l11[i][i2], uz[i2], acc);
-          uz[i] = ((zb >> i) & 1u) ? 0.0 : acc;
-          if (i > 0) *cell = acc;
-        }
-      }
-    }
-    __syncwarp();
-    // --------------------- 3. trailing update on the tensor cores, 8 x 8 tiles
-    switch ((NP - j1) / 8) {
-      case 7: tc_tiles<NP, NRHS, 7>(M, ord, pmap, zb, k0, lane); break;
-      case 6: tc_tiles<NP, NRHS, 6>(M, ord, pmap, zb, k0, lane); break;
-      case 5: tc_tiles<NP, NRHS, 5>(M, ord, pmap, zb, k0, lane); break;
-      case 4: tc_tiles<NP, NRHS, 4>(M, ord, pmap, zb, k0, lane); break;
-      case 3: tc_tiles<NP, NRHS, 3>(M, ord, pmap, zb, k0, lane); break;
-      case 2: tc_tiles<NP, NRHS, 2>(M, ord, pmap, zb, k0, lane); break;
-      case 1: tc_tiles<NP, NRHS, 1>(M, ord, pmap, zb, k0, lane); break;
-      default: tc_tiles<NP, NRHS, 0>(M, ord, pmap, zb, k0, lane); break;
-    }
-    __syncwarp();
+    // ------------------------------- 2. U12 and 3. the trailing update (tensor
+    // cores); a panel without a zero pivot (the common case) takes the forms without
+    // the zero-pivot selects
+    if (zb == 0u) tc_update<NP, NRHS, false>(M, ord, pmap, zb, k0, lane);
+    else tc_update<NP, NRHS, true>(M, ord, pmap, zb, k0, lane);
   }
 
-  if constexpr (NRHS > 0) seg_backsolve<T, NP, NRHS, false, 32>(M, ord, j, g);
+  if constexpr (NRHS > 0) tc_backsolve<NP, NRHS>(M, ord, pos, j, lane);
   if (j.live) {
     if (j.piv) {
 #pragma unroll
