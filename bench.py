@@ -901,12 +901,12 @@ def _stream_workload(a, world, rank, local, device, dist):
         Bs[j].copy_(B0)
     capi = _pkg("capi")
     ms, clk, _ = _timed(lambda i: graphs[i % pool].replay(), a, world, local, device, dist)
-    launches = 6 * a.steps  # histogram, scan, scatter and three drains per replay (counted at capture)
+    launches = 10 * a.steps  # histogram, scan, scatter and seven drains per replay (counted at capture)
     value = world * count / (ms * 1e-3)
     n64 = n.astype(np.int64)
     bytes_step = int((4 * (2 * n64 * n64 + 2 * n64 * nrhs) + 4 + np.where(kind == 1, 4 * n64, 0)).sum())
     flops_step = float((np.where(kind == 1, 2 * n64 ** 3 / 3, n64 ** 3 / 3) + 2 * n64 * n64 * nrhs).sum())
-    roof = _roof(bytes_step, ms, "stream_kernel<float> x3 drains (+ histogram, scan, scatter)", flops_step,
+    roof = _roof(bytes_step, ms, "stream_kernel<float> x7 drains (+ histogram, scan, scatter)", flops_step,
                  traffic_from_profiles("stream_f32", "stream_kernel"))
     extra = {"schedule": {"sched_bits": plan.sched, "tuned_ms": {str(k): round(v, 3) for k, v in plan.timings.items()}}}
     e2e = None

@@ -34,6 +34,15 @@
 namespace tsdx {
 namespace dev {
 
+// Hint: bring [p, p + bytes) into L2 (one bulk prefetch; the range is trimmed to
+// whole 16-byte units, as the instruction requires).
+__device__ __forceinline__ void prefetch_l2(const void* p, long long bytes) {
+  const unsigned long long a = reinterpret_cast<unsigned long long>(p);
+  const unsigned long long lo = (a + 15) & ~15ull, hi = (a + bytes) & ~15ull;
+  if (hi > lo)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"((unsigned)(hi - lo)) : "memory");
+}
+
 // GO overrides the lanes per matrix (32: one matrix per warp for any NP).
 template <class T, int NP, int NRHS, int GO = 0>
 struct BlkCfg {
@@ -126,6 +135,18 @@ __device__ __forceinline__ void seg_copy_out(const unsigned char* M, T* A, int n
   }
 }
 
+// y <- fma(-u, x, y) when p, else y unchanged: one predicated FMA (no select).
+__device__ __forceinline__ void fma_if(double& y, bool p, double u, double x) {
+  asm("{\n .reg .pred q;\n setp.ne.b32 q, %1, 0;\n @q fma.rn.f64 %0, %2, %3, %0;\n}"
+      : "+d"(y)
+      : "r"((int)p), "d"(-u), "d"(x));
+}
+__device__ __forceinline__ void fma_if(float& y, bool p, float u, float x) {
+  asm("{\n .reg .pred q;\n setp.ne.b32 q, %1, 0;\n @q fma.rn.f32 %0, %2, %3, %0;\n}"
+      : "+f"(y)
+      : "r"((int)p), "f"(-u), "f"(x));
+}
+
 // Stage the job's matrix (identity-padded to NP) and right-hand sides.
 template <class T, int NP, int NRHS, int GO>
 __device__ __forceinline__ void seg_load(unsigned char* M, const MatJob<T>& j, const Seg& g) {
@@ -174,30 +195,30 @@ __device__ __forceinline__ void seg_backsolve(unsigned char* M, const int* ord, 
     for (int c = 0; c < NRHS; ++c) yv[t][c] = at(pr, NP + c);
   }
   // a warp-uniform trip count (segments of one warp may hold different n); the
-  // identity-padded positions >= n carry zeros and change nothing
+  // identity-padded positions >= n carry zeros and change nothing. Rows above k take
+  // the update as a predicated FMA (U is read for every row; the address is inside
+  // the matrix); a row's y is final after its own step, so each row forms its
+  // x = y * RN(1/u_ii) once more at the end, the product that was broadcast.
 #pragma unroll 4
   for (int k = NP - 1; k >= 0; --k) {
     const int ks = k / G, kl = g.segbase + (k & (G - 1));
+    T d = dv[0];
+#pragma unroll
+    for (int t = 1; t < MR; ++t) d = (ks == t) ? dv[t] : d;
     T x[NRHS];
 #pragma unroll
     for (int c = 0; c < NRHS; ++c) {
-      T y = yv[0][c] * dv[0];
+      T y = yv[0][c];
 #pragma unroll
-      for (int t = 1; t < MR; ++t)
-        if (ks == t) y = yv[t][c] * dv[t];
-      x[c] = __shfl_sync(kFull, y, kl);
+      for (int t = 1; t < MR; ++t) y = (ks == t) ? yv[t][c] : y;
+      x[c] = __shfl_sync(kFull, y * d, kl);
     }
-    // branch-free: rows above k take the update, row k takes x, rows below keep y
-    // (U is read for every row; the address is inside the matrix)
 #pragma unroll
     for (int t = 0; t < MR; ++t) {
-      const int i = g.lsl + G * t;
+      const bool above = g.lsl + G * t < k;
       const T u = *reinterpret_cast<const T*>(ubase[t] + k * ustride);
 #pragma unroll
-      for (int c = 0; c < NRHS; ++c) {
-        const T upd = fma_(-u, x[c], yv[t][c]);
-        yv[t][c] = i < k ? upd : (i == k ? x[c] : yv[t][c]);
-      }
+      for (int c = 0; c < NRHS; ++c) fma_if(yv[t][c], above, u, x[c]);
     }
   }
   if (j.live && j.B) {
@@ -208,7 +229,7 @@ __device__ __forceinline__ void seg_backsolve(unsigned char* M, const int* ord, 
       T* brow = j.B + (long long)i * j.ldb + j.b0;
 #pragma unroll
       for (int c = 0; c < NRHS; ++c)
-        if (c < j.nrhs) brow[c] = yv[t][c];
+        if (c < j.nrhs) brow[c] = yv[t][c] * dv[t];
     }
   }
 }
@@ -602,9 +623,18 @@ __global__ void __launch_bounds__(WPC * 32, 1) blk_kernel(SolveArgs<T> p) {
   unsigned char* M = smem + warp * C::WARPB + (lane / G) * C::SEGB;
   const long long nn = (long long)p.n * p.n;
   const long long per_round = (long long)gridDim.x * WPC * S;
+  // warps own disjoint shared memory, so they run their rounds without a block barrier
   for (long long base = (long long)blockIdx.x * WPC * S; base < p.batch; base += per_round) {
-    __syncthreads();
     const long long m = base + (long long)warp * S + lane / G;
+    {
+      // this warp's next unit heads for L2 while this one is solved
+      const long long nxt = base + per_round + (long long)warp * S;
+      if (lane == 0 && nxt < p.batch) {
+        const long long cnt = (p.batch - nxt) < S ? (p.batch - nxt) : S;
+        prefetch_l2(p.A + nxt * nn, cnt * nn * (long long)sizeof(T));
+        if (p.B) prefetch_l2(p.B + nxt * (long long)p.n * p.ldb, cnt * (long long)p.n * p.ldb * (long long)sizeof(T));
+      }
+    }
     MatJob<T> j;
     j.live = m < p.batch && !(p.status && p.status[m] >= 0);
     if (!__any_sync(kFull, j.live)) continue;

@@ -38,14 +38,6 @@ __device__ __forceinline__ void dmma_m8n8k4(double2& c, double a, double b) {
       : "d"(a), "d"(b));
 }
 
-// Hint: bring [p, p + bytes) into L2 (one bulk prefetch; the range is trimmed to
-// whole 16-byte units, as the instruction requires).
-__device__ __forceinline__ void prefetch_l2(const void* p, long long bytes) {
-  const unsigned long long a = reinterpret_cast<unsigned long long>(p);
-  const unsigned long long lo = (a + 15) & ~15ull, hi = (a + bytes) & ~15ull;
-  if (hi > lo)
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"((unsigned)(hi - lo)) : "memory");
-}
 
 // ---- 1-D bulk copies (TMA, this GPU's own memory, no multicast) on an mbarrier
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -206,13 +198,6 @@ __device__ __forceinline__ void tc_update(unsigned char* M, const int* ord, cons
     default: tc_tiles<NP, NRHS, 0, ZB>(M, ord, pmap, zb, k0, lane); break;
   }
   __syncwarp();
-}
-
-// y <- fma(-u, x, y) when p, else y unchanged: one predicated FMA (no select).
-__device__ __forceinline__ void fma_if(double& y, bool p, double u, double x) {
-  asm("{\n .reg .pred q;\n setp.ne.b32 q, %1, 0;\n @q fma.rn.f64 %0, %2, %3, %0;\n}"
-      : "+d"(y)
-      : "r"((int)p), "d"(-u), "d"(x));
 }
 
 // Back substitution over physical rows: lane l solves its rows l and l + 32 (at

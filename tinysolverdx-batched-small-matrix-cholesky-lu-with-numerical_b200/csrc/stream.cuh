@@ -14,11 +14,11 @@
 // bucket = (kind, padded order NP in {8, 16, ..., 64}, right-hand-side class
 // {<= 2, <= 8}); each bucket is cut into work units of S matrices (S = 32/G
 // segments per warp for NP <= 32, as unit_size lists; or one warp per matrix when
-// the tuned schedule asks for it). Three persistent launches then drain the units
-// through global atomic queues, one per group of order classes (n 57..64, n 49..56,
-// n <= 48), largest orders first: each group's warps get the shared memory of its own
-// largest variant, so the smaller orders keep more warps per SM, and within a group the
-// SMs run mostly the same code variant with the smallest units filling the tail. Each
+// the tuned schedule asks for it). Seven persistent launches then drain the units
+// through global atomic queues, one per order class of 8 above order 16 and one for
+// n <= 16, largest orders first: each drain's warps get the shared memory of its own
+// largest variant, so the smaller orders keep more warps per SM, and each drain holds
+// only its class's few code variants (kind x right-hand-side class x packing). Each
 // unit is the same per-matrix body (blk.cuh) as the dense kernels, so the results are
 // bit-identical to them. The launches are capturable in a CUDA graph (no host
 // synchronisation; scratch passed in by the caller).

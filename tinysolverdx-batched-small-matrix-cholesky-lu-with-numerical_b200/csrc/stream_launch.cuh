@@ -1,5 +1,5 @@
 // Host side of the uneven stream (stream.cuh): counting sort into buckets + persistent
-// drains (one per order-class group), instantiated per element type in k_stream_f32.cu /
+// drains (one per order class above order 16, one for n <= 16), instantiated per element type in k_stream_f32.cu /
 // k_stream_f64.cu.
 #pragma once
 #include <cuda_runtime.h>
@@ -75,13 +75,19 @@ int run_stream(dev::StreamArgs<T> a, void* scratch, long long scratch_bytes, cud
     // the bucket cursors are dead after the scatter: zero them, they are the drains' queue heads
     e = cudaMemsetAsync(a.scratch + 2 * dev::kStreamBuckets, 0, dev::kStreamClasses * sizeof(int), st);
   }
-  // three drains, largest orders first: n 57..64, n 49..56, n <= 48 (shared memory per
-  // warp sized for each group, so the smaller orders keep more warps per SM)
+  // seven drains, largest orders first: one per order class of 8 above order 16, one for
+  // n <= 16. Shared memory per warp is sized for each class, so the smaller orders keep
+  // more warps per SM, and each drain carries only its class's code variants (one
+  // drain over n <= 48 carried about 40 and stalled on instruction fetch).
   if (e == cudaSuccess) rc = launch_drain<T, 7, 7>(a, st);
   if (e == cudaSuccess && !rc) rc = launch_drain<T, 6, 6>(a, st);
-  if (e == cudaSuccess && !rc) rc = launch_drain<T, 0, 5>(a, st);
+  if (e == cudaSuccess && !rc) rc = launch_drain<T, 5, 5>(a, st);
+  if (e == cudaSuccess && !rc) rc = launch_drain<T, 4, 4>(a, st);
+  if (e == cudaSuccess && !rc) rc = launch_drain<T, 3, 3>(a, st);
+  if (e == cudaSuccess && !rc) rc = launch_drain<T, 2, 2>(a, st);
+  if (e == cudaSuccess && !rc) rc = launch_drain<T, 0, 1>(a, st);
   if (e == cudaSuccess && !rc) {
-    launch_counter().fetch_add(6);
+    launch_counter().fetch_add(10);
     e = cudaGetLastError();
   }
   if (e != cudaSuccess) { set_cuda_error(e, "stream launch"); rc = -5; }

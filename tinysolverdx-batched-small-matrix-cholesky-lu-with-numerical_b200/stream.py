@@ -2,7 +2,7 @@
 
 Matrices of mixed order n (1..64), Cholesky (posv) and LU (gesv) mixed and 0..8
 right-hand sides each are packed back to back in flat buffers and solved by one
-counting sort into size buckets plus one persistent kernel that drains them
+counting sort into size buckets plus persistent kernels that drain them, one per order class
 (tsdx_cuda_solve_stream_* in include/tsdx_cuda.h). The results are bit-identical
 to the dense posv/gesv of each matrix.
 
@@ -193,7 +193,7 @@ class StreamPlan:
         return self.sched
 
     def capture(self):
-        """Capture one solve (memset, histogram, scan, scatter, memset, three drains) in a CUDA graph."""
+        """Capture one solve (memset, histogram, scan, scatter, memset, seven drains) in a CUDA graph."""
         s = torch.cuda.Stream(self.device)
         s.wait_stream(torch.cuda.current_stream(self.device))
         with torch.cuda.stream(s):
