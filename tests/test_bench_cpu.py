@@ -93,3 +93,40 @@ def test_both_arms_describe_the_same_config():
         batch = b.WORKLOADS[name][2]
         c = b.describe(name, batch, 1)
         assert c["global_batch"] == batch and c["batch_per_gpu"] == batch and c["parallelism"]
+
+
+def test_dense_kernel_follows_the_launch_routing(monkeypatch):
+    """bench.py names the kernel that csrc/launch.cuh launches: float64 LU on the
+    tensor-core kernel from padded order 32 (even orders up to 64, every order up to
+    48), the two-warp kernels for odd orders above 48, blk_kernel otherwise."""
+    b = _bench()
+    monkeypatch.delenv("TSDX_LU_KERNEL", raising=False)
+    for n in (25, 32, 33, 41, 47, 48, 50, 56, 58, 64):
+        assert b.dense_kernel("gesv", n, "f64")[0] == "tc_kernel", n
+    for n in (49, 51, 55):
+        assert b.dense_kernel("gesv", n, "f64")[0] == "blk2_kernel", n
+    for n in (57, 61, 63):
+        assert b.dense_kernel("gesv", n, "f64")[0] == "blk3_kernel", n
+    for kind, n, dt in (("gesv", 24, "f64"), ("gesv", 64, "f32"), ("gesv", 32, "f32"), ("posv", 16, "f64"),
+                        ("posv", 64, "f64")):
+        assert b.dense_kernel(kind, n, dt)[0] == "blk_kernel", (kind, n, dt)
+    monkeypatch.setenv("TSDX_LU_KERNEL", "smem")
+    assert b.dense_kernel("gesv", 64, "f64")[0] == "blk3_kernel"
+    monkeypatch.setenv("TSDX_LU_KERNEL", "tc")
+    assert b.dense_kernel("gesv", 63, "f64")[0] == "tc_kernel"
+
+
+def test_roofline_traffic_comes_from_the_routed_kernels_profile(monkeypatch):
+    """A dense line's roofline traffic is read from profiles/<kernel>__<workload>.md of
+    the kernel that runs; the default workload has one."""
+    b = _bench()
+    monkeypatch.delenv("TSDX_LU_KERNEL", raising=False)
+    prof = ROOT / "profiles"
+    for name, (kind, n, _b, _r, dt, *_rest) in b.WORKLOADS.items():
+        stem, _ = b.dense_kernel(kind, n, dt)
+        cited = b.traffic_from_profiles(name, stem)
+        others = [p.name for p in prof.glob(f"*__{name}.md") if not p.name.startswith(stem + "__")]
+        assert not others, f"{name}: profiles of kernels that do not run: {others}"
+        if (prof / f"{stem}__{name}.md").exists():
+            assert cited is not None and cited > 0, name
+    assert b.traffic_from_profiles("gesv_f64_n64", "tc_kernel") > 0
