@@ -168,7 +168,8 @@ int launch_blk(const SolveArgs<T>& a, cudaStream_t st) {
   // float64 LU from padded order 32 on: the tensor-core trailing update. Measured on
   // B200 against the shared-memory kernels (65,536-262,144 matrices, 4 right-hand
   // sides, M solves/s): n=25 77.1 vs 68.1, n=32 93.0 vs 65.3, n=40 38.0 vs 33.3,
-  // n=48 26.8 vs 23.1, n=56 18.2 vs 16.7, n=64 15.3 vs 12.9. Odd orders above 48
+  // n=48 26.8 vs 23.1, n=56 18.2 vs 16.7, n=64 15.3 vs 12.9 (its later changes took
+  // n=64 to 16.9: the back substitution, the winner record and U12). Odd orders above 48
   // stay on the shared-memory kernels (n=61 11.6 vs 12.3): their rows are not whole
   // 16-byte units, so the matrix cannot arrive by bulk copies.
   if constexpr (!CHOL && sizeof(T) == 8 && NP >= 32) {
