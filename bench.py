@@ -818,9 +818,10 @@ def _ir_workload(a, world, rank, local, device, dist):
     extra["bwd_max_ratio_vs_plain_fp64"] = round(errs["selector"]["max"] / errs["plain_fp64"]["max"], 3)
     extra["speedup_vs_plain_fp64"] = round(value / world / extra["plain_fp64"]["solves_per_s"], 3)
     bytes_step = batch * (8 * (n * n + 2 * n) + 4)
-    routed = "every matrix routed to fp64 by the calibrated policy: blk2_kernel x-only" if tiers.get("fp64") == batch \
-        else "ir_kernel<64> + features + mlp_forward + fp64 fallback"
-    roof = _roof(bytes_step, ms, routed, traffic=traffic_from_profiles("ir_n64", "ir_kernel"))
+    all_fp64 = tiers.get("fp64") == batch
+    routed = ("every matrix routed to fp64 by the calibrated policy: tc_kernel (LU) and blk_kernel (Cholesky), "
+              "x only") if all_fp64 else "ir_kernel<64> + features + mlp_forward + fp64 fallback"
+    roof = _roof(bytes_step, ms, routed, traffic=None if all_fp64 else traffic_from_profiles("ir_n64", "ir_kernel"))
     # end to end: pinned host A and b in, x and info out, every step
     e2e = None
     if not a.skip_e2e:
