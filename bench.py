@@ -1005,12 +1005,13 @@ def _selector_workload(a, world, rank, local, device, dist):
         extra[name] = {"solves_per_s": round(count / (t * 1e-3), 1), "ms": round(t, 3)}
         if tier != 3:
             extra[name]["fp64_fallbacks"] = fall
-    fall = 0
+    fall = nfp64 = 0
     for gr in groups:
         x = gr["b"].clone()
         _, status, _, tier = s.solve(gr["A"], x, gr["spd"])
         bw.setdefault("selector", []).append(_bwd(gr["A"], x, gr["b"]))
         fall += int(((tier < 3) & (status < 0)).sum().item())
+        nfp64 += int((tier == 3).sum().item())
     extra["selector_fp64_fallbacks"] = fall
     errs = {k: _stats(torch.cat(v)) for k, v in bw.items()}
     extra["backward_error"] = errs
@@ -1018,7 +1019,9 @@ def _selector_workload(a, world, rank, local, device, dist):
     extra["speedup_vs_fixed_fp16"] = round(value / world / extra["fixed_fp16"]["solves_per_s"], 3)
     extra["speedup_vs_fixed_fp32"] = round(value / world / extra["fixed_fp32"]["solves_per_s"], 3)
     nsum = sum(gr["count"] * (8 * (gr["n"] ** 2 + 2 * gr["n"]) + 4) for gr in groups)
-    roof = _roof(nsum, ms, "ir_kernel (+ features, mlp_forward, fp64 fallback)", traffic=None)
+    routed = ("every matrix routed to fp64 by the calibrated policy: the plain fp64 kernels of each order, x only"
+              if nfp64 == count else "ir_kernel (+ features, mlp_forward, fp64 fallback)")
+    roof = _roof(nsum, ms, routed, traffic=None)
     cfg = {"workload": SPECIAL["selector"], "global_batch": world * count, "batch_per_gpu": count,
            "parallelism": f"evaluation set sharded over {world} GPU(s), no collective",
            "l2": "inputs larger than L2 (13 GB of A per step)", "selector": f"{PKG_NAME}/selector_weights.npz"}
