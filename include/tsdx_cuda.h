@@ -180,10 +180,12 @@ int tsdx_cuda_adam_step(float* params, const float* grad, float* m, float* v, in
  *   info[i]      LAPACK-style info; -1 for an entry outside the supported sizes
  * Factors, pivots, info and X are bit-identical to the dense tsdx_cuda_posv/gesv_*.
  * The matrices are counting-sorted into buckets (kind, padded order, right-hand-side
- * class) and drained by one persistent kernel through an atomic queue; the launches
- * are stream-ordered and can be captured in a CUDA graph. sched: bit 0 / bit 1 run
- * the n <= 8 / n <= 16 buckets one matrix per warp instead of packing 4 / 2 per warp
- * (chosen by the autotuner of the Python layer). scratch: device memory of at least
+ * class) and drained by persistent kernels, one per order class of 8 above order 16
+ * and one for n <= 16, each through its own atomic queue; the launches are
+ * stream-ordered and can be captured in a CUDA graph. sched: bit c (c = 0..3, orders
+ * up to 8, 16, 24, 32) runs that class one matrix per warp instead of packing several
+ * per warp (8 Cholesky or 4 LU up to order 8, 4 up to 16, 4 (float32) or 2 (float64)
+ * up to 24, 2 up to 32); the autotuner of the Python layer chooses it. scratch: device memory of at least
  * tsdx_cuda_stream_scratch_bytes(count) bytes, or NULL to allocate it on the stream. */
 int64_t tsdx_cuda_stream_scratch_bytes(int64_t count);
 int tsdx_cuda_solve_stream_f32(float* A, const int64_t* aoff, float* B, const int64_t* boff, int* piv,
